@@ -1,0 +1,85 @@
+"""Build the in-tree native libraries.
+
+libadb_b200.so   the CUDA join library (sm_100a only), from alliancedb_b200/csrc/*.cu
+liboracle.so     the CPU checker used by tests (oracle/adb_oracle.c), built beside it
+
+Run as ``python -m alliancedb_b200.build`` or through ``__graft_entry__.build()``.
+Objects go to _build/ (not committed); the shared libraries stay in the tree
+so they travel with the repository snapshot.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent.parent
+PKG = ROOT / "alliancedb_b200"
+CSRC = PKG / "csrc"
+BUILD = ROOT / "_build"
+LIB = PKG / "libadb_b200.so"
+ORACLE_LIB = ROOT / "oracle" / "liboracle.so"
+
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
+           "--expt-relaxed-constexpr", "-I", str(ROOT / "include")]
+
+
+def _run(cmd: list[str]) -> None:
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError(f"build step failed: {' '.join(cmd)}")
+
+
+def _newer(src: Path, dst: Path, deps: list[Path]) -> bool:
+    if not dst.exists():
+        return True
+    t = dst.stat().st_mtime
+    return src.stat().st_mtime > t or any(d.stat().st_mtime > t for d in deps)
+
+
+def build_cuda(verbose: bool = False) -> Path:
+    BUILD.mkdir(exist_ok=True)
+    sources = sorted(CSRC.glob("*.cu"))
+    headers = sorted(CSRC.glob("*.cuh")) + sorted((ROOT / "include").rglob("*.h"))
+    objs = []
+    jobs = []
+    for src in sources:
+        obj = BUILD / (src.stem + ".o")
+        objs.append(obj)
+        if _newer(src, obj, headers):
+            cmd = [NVCC, *ARCH, *NVFLAGS, "-c", str(src), "-o", str(obj)]
+            if verbose:
+                cmd += ["-Xptxas", "-v"]
+            jobs.append(cmd)
+    with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
+        list(ex.map(_run, jobs))
+    if jobs or not LIB.exists():
+        tmp = LIB.with_suffix(".so.tmp")
+        _run([NVCC, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lpthread"])
+        os.replace(tmp, LIB)
+    return LIB
+
+
+def build_oracle() -> Path:
+    src = ROOT / "oracle" / "adb_oracle.c"
+    hdr = ROOT / "oracle" / "adb_oracle.h"
+    if _newer(src, ORACLE_LIB, [hdr]):
+        tmp = ORACLE_LIB.with_suffix(".so.tmp")
+        _run(["gcc", "-O2", "-std=c11", "-shared", "-fPIC", "-o", str(tmp), str(src)])
+        os.replace(tmp, ORACLE_LIB)
+    return ORACLE_LIB
+
+
+def build_all(verbose: bool = False) -> None:
+    build_oracle()
+    build_cuda(verbose)
+
+
+if __name__ == "__main__":
+    build_all(verbose="-v" in sys.argv)
+    print(LIB)

@@ -1,0 +1,67 @@
+// engine.cuh -- host-side context of the join library: device, stream, events,
+// a grow-only device workspace, and the status/error plumbing of the C ABI.
+#pragma once
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "adb_common.cuh"
+
+namespace adb {
+
+void set_error(const char *fmt, ...);
+
+#define ADB_CK(call)                                                                      \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess) {                                                          \
+            ::adb::set_error("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_),      \
+                             __FILE__, __LINE__);                                         \
+            return e_ == cudaErrorMemoryAllocation ? ADB_ERR_OOM : ADB_ERR_DEVICE;        \
+        }                                                                                 \
+    } while (0)
+
+#define ADB_TRY(expr)                      \
+    do {                                   \
+        int s_ = (expr);                   \
+        if (s_ != ADB_OK) return s_;       \
+    } while (0)
+
+// Bump allocator over one cached device buffer.  reserve() grows the buffer
+// (free + malloc) only when a call needs more than the current capacity, so
+// repeated joins of one size allocate nothing.
+struct Workspace {
+    char *base = nullptr;
+    size_t cap = 0;
+    size_t off = 0;
+    int reserve(size_t bytes);
+    void reset() { off = 0; }
+    template <class T>
+    T *take(size_t count) {
+        size_t bytes = (count * sizeof(T) + 255) & ~(size_t)255;
+        T *p = reinterpret_cast<T *>(base + off);
+        off += bytes;
+        return p;
+    }
+    static size_t need(size_t count, size_t elem) { return (count * elem + 255) & ~(size_t)255; }
+    void release();
+};
+
+struct Context {
+    int device = -1;
+    int num_sms = kNumSMs;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[8] = {};
+    Workspace ws;
+    unsigned long long *h_res = nullptr;   // pinned: [0] count [1] checksum [2] err [3] mat_n ...
+    bool attrs_set = false;
+    int kernels = 0;                       // kernels launched by the current call
+};
+
+// The per-device context (created on first use).  Returns nullptr and sets
+// the error if no device is usable.
+Context *ctx_get(int *status);
+
+}  // namespace adb

@@ -1,0 +1,45 @@
+// joins.cuh -- device-resident join drivers shared by the C ABI and the
+// batched/served paths.  Each driver: scratch size for a call, then the
+// launch sequence on ctx->stream.  Results land in acc[0] (count) and acc[1]
+// (checksum) of a device accumulator the caller zeroed; acc[2] is the error
+// word (a timed-out device wait sets it), acc[3] the materialised count.
+#pragma once
+
+#include "engine.cuh"
+
+namespace adb {
+
+struct DevJoin {
+    const uint64_t *R;
+    uint64_t nR;
+    const uint64_t *S;
+    uint64_t nS;
+    uint64_t *mat = nullptr;      // optional <S-key, S-payload> output
+    uint64_t mat_cap = 0;
+};
+
+struct JoinTimes {
+    float ms[4] = {0, 0, 0, 0};
+};
+
+enum class Family { Radix, RadixHist, Npo, SortMerge, Shj, Pmj, Unsupported };
+
+// ---- radix (PRO / RJ_st / PRH / PRHO) ----
+int radix_bits_for(uint64_t nR, int requested);
+size_t radix_scratch(uint64_t nR, uint64_t nS, int bits, int num_sms);
+int run_radix(Context *ctx, const DevJoin &j, bool hist_table, int bits, unsigned long long *acc);
+
+// ---- NPO / NPO_st ----
+size_t npo_scratch(uint64_t nR);
+int run_npo(Context *ctx, const DevJoin &j, unsigned long long *acc);
+
+// ---- m-way / m-pass ----
+size_t smj_scratch(uint64_t nR, uint64_t nS, int num_sms);
+int run_smj(Context *ctx, const DevJoin &j, int part_fanout, bool multipass, unsigned long long *acc);
+
+// ---- eager SHJ / PMJ over one window given as arrival-ordered relations ----
+size_t eager_scratch(uint64_t nR, uint64_t nS, Family fam, uint64_t batch);
+int run_eager(Context *ctx, const DevJoin &j, Family fam, int model, uint64_t batch, int nthreads,
+              int group_size, int progressive_step, uint64_t seed, unsigned long long *acc);
+
+}  // namespace adb

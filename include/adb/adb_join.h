@@ -1,0 +1,192 @@
+/*
+ * adb_join.h -- C ABI of the B200 join library (libadb_b200.so).
+ *
+ * This is the drop-in boundary for AllianceDB's join hot path.  The reference
+ * dispatches joins through a name -> function table:
+ *   hashing:  algo_t{name, result_t *(*)(relation_t *, relation_t *, param_t)}
+ *             (hashing/benchmark.h:53-57, table hashing/main.cpp:306-338,
+ *              called at hashing/benchmark.cpp:244-247)
+ *   sorting:  algo_t{name, result_t *(*)(relation_t *, relation_t *, joinconfig_t *,
+ *                    int exp_id, int window_size, int gap)}
+ *             (sorting/main.cpp:420-425, table :481-486, called at :752-758)
+ * adb_join() takes the same algorithm names and the same relations (arrays of
+ * 8-byte {payload @0, key @4} tuples, hashing/utils/types.h:67-70) and returns
+ * the reference's result (the match count, result_t.totalresults,
+ * hashing/utils/types.h:98-102) plus an order-independent 64-bit checksum over
+ * the matched (key, r_payload, s_payload) triples:
+ *     a = (u64)key << 32 | r_payload,  b = (u64)s_payload << 32 | key,
+ *     H = fmix64(a ^ fmix64(b)),  checksum = sum of H mod 2^64,
+ * fmix64 being the SplitMix64 finalizer.
+ *
+ * Differences from the reference, all deliberate:
+ *  - inputs are never modified (the reference's PRO overwrites R and S,
+ *    hashing/joins/parallel_radix_join.cpp:1176-1181);
+ *  - errors are status codes, never exit() (the reference exits on malloc or
+ *    barrier failure, :47-64);
+ *  - keys are unsigned 32-bit and every value, 0 and 0xFFFFFFFF included, is a
+ *    valid key.
+ *
+ * All functions are thread-compatible, not thread-safe: one host thread per
+ * library context (the library keeps one context per device).
+ */
+#ifndef ADB_JOIN_H
+#define ADB_JOIN_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* hashing/utils/types.h:67-70 and sorting/utils/types.h:63-67 */
+typedef struct adb_tuple {
+    uint32_t payload;
+    uint32_t key;
+} adb_tuple;
+
+/* Timestamped stream tuple (the reference keeps ts in relation_payload_t,
+ * hashing/utils/types.h:83-88; here it travels beside the tuple). */
+typedef struct adb_stream_tuple {
+    uint64_t ts_ms;
+    adb_tuple t;
+} adb_stream_tuple;
+
+typedef enum adb_status {
+    ADB_OK = 0,
+    ADB_ERR_ARG = 1,         /* bad argument: NULL pointer, unknown algorithm, size out of range */
+    ADB_ERR_OOM = 2,         /* device or pinned-host allocation failed */
+    ADB_ERR_DEVICE = 3,      /* a CUDA call failed; the message says which */
+    ADB_ERR_TIMEOUT = 4,     /* a bounded device wait ran out */
+    ADB_ERR_UNSUPPORTED = 5, /* name known to the reference but not provided (see adb_algo_info) */
+    ADB_ERR_BUSY = 6,        /* admission refused: over the device-memory budget */
+    ADB_ERR_NO_DEVICE = 7    /* no CUDA device, or the kernels were not built for it */
+} adb_status;
+
+/* Subset of the reference's param_t (hashing/benchmark.h:59-112) that the join
+ * functions read, plus the GPU tuning knobs.  Zero means "default" for every
+ * field; adb_params_default() fills the reference's defaults. */
+typedef struct adb_join_params {
+    uint32_t nthreads;          /* param_t.nthreads: worker count of the distribution model (JM/JB/JBCR) */
+    int32_t window_size;        /* param_t.window_size, ms (eager joins) */
+    int32_t step_size_r;        /* param_t.step_sizeR, tuples per interval */
+    int32_t step_size_s;        /* param_t.step_sizeS */
+    int32_t interval;           /* param_t.interval, ms */
+    int32_t group_size;         /* param_t.group_size, JBCR groups (-G) */
+    int32_t progressive_step;   /* param_t.progressive_step, PMJ run size in % of each side */
+    int32_t merge_step;         /* param_t.merge_step, PMJ runs merged per step */
+    int32_t radix_bits;         /* PRO/PRH/RJ fan-out bits; 0 = chosen from |R| */
+    int32_t part_fanout;        /* joinconfig_t.PARTFANOUT for m-way/m-pass; 0 = chosen */
+    int32_t materialize;        /* 1: also write <S-key, S-payload> per match (JOIN_RESULT_MATERIALIZE) */
+    int32_t batch_tuples;       /* eager joins: arrival micro-batch in tuples per side; 0 = 1 ms of stream */
+    uint64_t seed;              /* JBCR's random split of S */
+} adb_join_params;
+
+typedef struct adb_join_result {
+    uint64_t count;             /* result_t.totalresults */
+    uint64_t checksum;          /* sum of H over the matched pairs, mod 2^64 */
+    int32_t status;             /* adb_status */
+    int32_t kernels;            /* kernels this call launched */
+    float ms_device;            /* device time of the join, CUDA events on the library stream */
+    float ms_phase[4];          /* partition / build / probe / reduce (algorithm-specific split) */
+    float ms_h2d;               /* host->device copy time (adb_join only) */
+    uint64_t materialized;      /* tuples written to the materialisation buffer */
+} adb_join_result;
+
+void adb_params_default(adb_join_params *p);
+
+/* Last error message of this thread (static storage, never NULL). */
+const char *adb_last_error(void);
+const char *adb_version(void);
+
+/* Number of algorithm names, and the i-th name with its status:
+ * 1 = provided, 0 = known to the reference but not provided. */
+int adb_algo_count(void);
+const char *adb_algo_name(int i, int *provided);
+
+/* Join two host-resident relations: copies R and S to the device (inside the
+ * call), joins, and reads back the result.  Replaces the algos[] entry
+ * `name`.  R and S are not modified. */
+int adb_join(const char *algo, const adb_tuple *R, uint64_t nR, const adb_tuple *S, uint64_t nS,
+             const adb_join_params *p, adb_join_result *out);
+
+/* Join two device-resident relations on `stream` (a cudaStream_t, NULL = the
+ * library stream).  Returns after the result is on the host. */
+int adb_join_device(const char *algo, const adb_tuple *dR, uint64_t nR, const adb_tuple *dS,
+                    uint64_t nS, const adb_join_params *p, adb_join_result *out, void *stream);
+
+/* Materialising join (JOIN_RESULT_MATERIALIZE, hashing/joins/common_functions.cpp:255-258):
+ * writes one <S-key, S-payload> tuple per match into dOut (device, capacity
+ * `cap` tuples) in an unspecified order; out->materialized = matches written,
+ * out->count = all matches (count > cap means the buffer was too small). */
+int adb_join_materialize_device(const char *algo, const adb_tuple *dR, uint64_t nR,
+                                const adb_tuple *dS, uint64_t nS, const adb_join_params *p,
+                                adb_tuple *dOut, uint64_t cap, adb_join_result *out, void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* Eager stream joins (SHJ_* / PMJ_*) over tumbling windows.              */
+/* ---------------------------------------------------------------------- */
+
+/* Per-window result of a windowed stream join. */
+typedef struct adb_window_result {
+    uint64_t window_start_ms;
+    uint64_t n_r, n_s;
+    uint64_t count, checksum;
+    float latency_ms;           /* close-of-window -> result on host, device clock */
+    float reserved;
+} adb_window_result;
+
+/* Join two timestamp-ordered streams in tumbling windows of p->window_size
+ * ms.  Tuples are fed to the device in arrival micro-batches of
+ * p->batch_tuples (default: one millisecond of stream) and each batch is
+ * joined on arrival against the window's device-resident state (eager
+ * join).  Writes up to max_windows results; *n_windows = windows seen. */
+int adb_stream_join(const char *algo, const adb_stream_tuple *R, uint64_t nR,
+                    const adb_stream_tuple *S, uint64_t nS, const adb_join_params *p,
+                    adb_window_result *windows, uint64_t max_windows, uint64_t *n_windows);
+
+/* ---------------------------------------------------------------------- */
+/* Batched windows: many independent R/S pairs joined in one launch.      */
+/* ---------------------------------------------------------------------- */
+
+/* Window w is R[r_off[w] .. r_off[w+1]) joined with S[s_off[w] .. s_off[w+1]),
+ * all device-resident (offsets are host arrays of n_windows+1 entries).
+ * mode 0 = one persistent launch sequence for all windows (work stealing over
+ * (window, partition) items); mode 1 = one launch sequence per window. */
+int adb_batch_join_device(const adb_tuple *dR, const uint64_t *r_off, const adb_tuple *dS,
+                          const uint64_t *s_off, uint32_t n_windows, int mode,
+                          uint64_t *counts, uint64_t *checksums, float *ms_device, void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* Device memory helpers for callers without a CUDA runtime of their own. */
+/* ---------------------------------------------------------------------- */
+int adb_device_alloc(void **ptr, size_t bytes);
+int adb_device_free(void *ptr);
+int adb_host_alloc_pinned(void **ptr, size_t bytes);
+int adb_host_free_pinned(void *ptr);
+int adb_memcpy_h2d(void *dst, const void *src, size_t bytes);
+int adb_memcpy_d2h(void *dst, const void *src, size_t bytes);
+int adb_device_sync(void);
+/* Releases the cached device workspace (it is re-created on the next join). */
+int adb_release_workspace(void);
+
+/* ---------------------------------------------------------------------- */
+/* Seeded synthetic relations (the generator of the benchmark configs).   */
+/* Counter-based: element i depends only on (seed, i), so host and device */
+/* produce identical arrays.  Arrays may be host or device pointers as    */
+/* named.                                                                 */
+/* ---------------------------------------------------------------------- */
+
+/* R: key = 1 + perm_seed(i) (a permutation of 1..n), payload = i. */
+int adb_gen_pk(adb_tuple *R, uint64_t n, uint64_t seed, int on_device);
+/* S: payload = j, key = R.key[idx_j] with idx_j Zipf(theta) over 0..nR-1 through a
+ * seeded rank permutation (theta = 0: uniform).  idx (may be NULL) receives idx_j. */
+int adb_gen_fk(adb_tuple *S, uint64_t nS, const adb_tuple *R, uint64_t nR, double theta,
+               uint64_t seed, uint32_t *idx, int on_device);
+/* Non-unique: key = 1 + uniform(seed, i) % key_range, payload = i. */
+int adb_gen_uniform(adb_tuple *T, uint64_t n, uint64_t key_range, uint64_t seed, int on_device);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ADB_JOIN_H */
