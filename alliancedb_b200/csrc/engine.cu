@@ -228,21 +228,23 @@ static int join_device_core(Context *ctx, const AlgoEntry *a, DevJoin j, const a
     ctx->ws.off = pre_bytes;
     unsigned long long *acc = ctx->ws.take<unsigned long long>(4);
     ADB_CK(cudaMemsetAsync(acc, 0, 4 * sizeof(unsigned long long), st));
-    ADB_CK(cudaEventRecord(ctx->ev[0], st));
-    ADB_CK(cudaEventRecord(ctx->ev[1], st));
+    // phase events: ev[0] start; drivers record ev[1..3] at their phase
+    // boundaries (radix: after histograms, after scatter, before the join
+    // kernel); ev[6] end.  Unrecorded boundaries collapse onto the start.
+    for (int k = 0; k < 4; k++) ADB_CK(cudaEventRecord(ctx->ev[k], st));
     if (j.nR && j.nS) ADB_TRY(dispatch(ctx, a, j, p, acc));
-    ADB_CK(cudaEventRecord(ctx->ev[2], st));
+    ADB_CK(cudaEventRecord(ctx->ev[6], st));
     ADB_CK(cudaMemcpyAsync(ctx->h_res, acc, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     ADB_CK(cudaStreamSynchronize(st));
-    float t0 = 0, t1 = 0;
-    ADB_CK(cudaEventElapsedTime(&t0, ctx->ev[0], ctx->ev[1]));
-    ADB_CK(cudaEventElapsedTime(&t1, ctx->ev[1], ctx->ev[2]));
+    float t[4] = {0, 0, 0, 0}, tot = 0;
+    ADB_CK(cudaEventElapsedTime(&tot, ctx->ev[0], ctx->ev[6]));
+    for (int k = 0; k < 3; k++) ADB_CK(cudaEventElapsedTime(&t[k], ctx->ev[k], ctx->ev[k + 1]));
+    ADB_CK(cudaEventElapsedTime(&t[3], ctx->ev[3], ctx->ev[6]));
     out->count = ctx->h_res[0];
     out->checksum = ctx->h_res[1];
     out->materialized = std::min<uint64_t>(ctx->h_res[3], j.mat_cap);
-    out->ms_phase[0] = t0;
-    out->ms_phase[1] = t1;
-    out->ms_device = t0 + t1;
+    for (int k = 0; k < 4; k++) out->ms_phase[k] = t[k];
+    out->ms_device = tot;
     out->kernels = ctx->kernels;
     if (ctx->h_res[2]) {
         set_error("a bounded device wait ran out (error word %llu)", ctx->h_res[2]);

@@ -31,6 +31,8 @@ int run_npo(Context *ctx, const DevJoin &j, unsigned long long *acc) {
     };
     npo_build<<<blocks(j.nR), threads, 0, st>>>(j.R, j.nR, table, l2, sent, reinterpret_cast<int *>(acc + 2));
     ADB_CK(cudaEventRecord(ctx->ev[1], st));
+    ADB_CK(cudaEventRecord(ctx->ev[2], st));
+    ADB_CK(cudaEventRecord(ctx->ev[3], st));
     if (j.mat)
         npo_probe<true><<<blocks(j.nS), threads, 0, st>>>(j.S, j.nS, table, l2, sent, acc, j.mat, acc + 3, j.mat_cap);
     else

@@ -58,11 +58,13 @@ int run_radix(Context *ctx, const DevJoin &j, bool hist_table, int bits, unsigne
     part_hist<<<dim3(G, 2), kPartThreads, F * 4, st>>>(rp, df, hist, G);
     part_scan_rows<<<(2 * F + 7) / 8, 256, 0, st>>>(hist, totals, F, G);
     part_scan_totals<<<2, 1024, 0, st>>>(totals, starts, F);
+    ADB_CK(cudaEventRecord(ctx->ev[1], st));
     part_scatter<<<dim3(G, 2), kPartThreads, scatter_smem(F), st>>>(rp, df, hist, starts, G);
     ADB_CK(cudaGetLastError());
-    ADB_CK(cudaEventRecord(ctx->ev[1], st));
+    ADB_CK(cudaEventRecord(ctx->ev[2], st));
 
     make_items<<<1, 1024, 0, st>>>(starts, F, items_off, ctr, kRCap, kSChunk);
+    ADB_CK(cudaEventRecord(ctx->ev[3], st));
     JoinArgs a;
     a.R = pR; a.S = pS; a.starts = starts; a.items_off = items_off;
     a.n_items = ctr; a.work_counter = ctr + 1;

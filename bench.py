@@ -1,0 +1,332 @@
+"""Benchmark of the B200 join hot path (one JSON line on rank 0).
+
+Workload (N=1): PRO radix hash join, |R| = |S| = 2^27 tuples of (u32 key, u32
+payload); R keys a seeded permutation of 1..|R|, S keys drawn uniformly from
+R's keys (the foreign-key case of the NPO / m-way config at 2^27, Zipf theta 0),
+payload = row index; output the match count plus the order-independent 64-bit
+checksum.  A step = one join of the full relations.
+
+  value   join input tuples/s, inputs resident in HBM (2 GiB, larger than the
+          126 MB L2, so no flush is needed between steps), CUDA events on the
+          stream the library launches on, max over ranks
+  e2e     the same metric through adb_join with pinned host buffers: the
+          host->device copy of R and S and the read-back of the result are
+          inside every timed step
+  roofline  the dominant kernel's algorithmic bytes / its device time vs the
+          measured HBM copy bandwidth (MEASURED_PEAKS.json)
+  cpu_baseline  the CPU join timed on this host (rank 0, N=1) on a bounded
+          sample of the workload
+
+`--impl reference` times the reference CPU join of the same workload instead:
+the reference's own code compiled from its sources (oracle/_ref) when present,
+otherwise the oracle's CPU restatement, using the host's threads.
+
+Multi-GPU (`--gpus N` under torchrun): every rank joins its own R/S pair of the
+same size (independent windows, no exchange): weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+# algorithmic bytes per input tuple of each family (whole pipeline)
+ALG_BYTES = {"PRO": 24, "RJ_st": 24, "PRH": 24, "PRHO": 24, "NPO": 16, "NPO_st": 16,
+             "m-way": 24, "m-pass": 24, "m-way+skew": 24}
+# dominant-phase index and its algorithmic bytes per input tuple
+PHASE_BYTES = {"radix": {1: 16, 3: 8, 0: 8}, "npo": {0: 8, 3: 8}}
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d["hbm_gbs"], "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms in the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"], f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def load_traffic(kernel: str):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
+    f = ROOT / "profiles" / "traffic.json"
+    if f.exists():
+        d = json.loads(f.read_text())
+        return d.get(kernel)
+    return None
+
+
+def make_inputs(adb, n: int, theta: float, seed: int):
+    R = adb.gen_pk(n, seed)
+    S = adb.gen_fk(n, R, theta, seed + 1)
+    return R, S
+
+
+def cpu_baseline_port(algo: str, n_sample: int, budget_s: float):
+    """Time the oracle's CPU restatement (single thread) on samples of the workload."""
+    import alliancedb_b200 as adb
+    from tests.oracle_bind import Oracle
+    o = Oracle()
+    fn = {"PRO": o.pro, "RJ_st": o.pro, "PRH": o.prh, "PRHO": o.prh, "NPO": o.npo, "NPO_st": o.npo,
+          "m-way": o.smj, "m-pass": o.smj, "m-way+skew": o.smj}[algo]
+    R, S = make_inputs(adb, n_sample, 0.0, 101)
+    done, t_tot, reps = 0, 0.0, 0
+    while t_tot < budget_s or reps < 1:
+        t0 = time.perf_counter()
+        cnt, _ = fn(R, S)
+        t_tot += time.perf_counter() - t0
+        assert cnt == n_sample
+        done += 2 * n_sample
+        reps += 1
+    return done / t_tot, reps
+
+
+def reference_arm(args):
+    """--impl reference: the reference's CPU join on this host."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    ref = ROOT / "oracle" / "_ref" / "adb_ref_bench"
+    n_sample = 1 << 24 if args.log2n >= 24 else 1 << args.log2n
+    if ref.exists():
+        threads = os.cpu_count() or 1
+        vals = []
+        for _ in range(args.warmup):
+            subprocess.run([str(ref), args.algo, str(n_sample), str(threads), "1"], check=True, capture_output=True)
+        for _ in range(args.steps):
+            out = subprocess.run([str(ref), args.algo, str(n_sample), str(threads), "1"], check=True,
+                                 capture_output=True, text=True).stdout
+            vals.append(json.loads(out.strip().splitlines()[-1])["tuples_per_s"])
+        value, kind, cores = statistics.median(vals), "reference", threads
+        sample = f"{args.algo} |R|=|S|=2^{n_sample.bit_length() - 1}, reference code, {threads} threads, join call only"
+    else:
+        vals = []
+        for _ in range(args.steps):
+            v, _ = cpu_baseline_port(args.algo, n_sample, 2.0)
+            vals.append(v)
+        value, kind, cores = statistics.median(vals), "port", 1
+        sample = f"{args.algo} |R|=|S|=2^{n_sample.bit_length() - 1}, oracle restatement, 1 thread"
+    line = {"impl": "reference", "metric": "join input tuples/s", "value": value, "unit": "tuples/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32 key/payload", "data": "synthetic",
+            "config": workload_config(args),
+            "cpu_baseline": {"value": value, "unit": "tuples/s", "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": "tuples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(args):
+    return {"workload": f"{args.algo} join |R|=|S|=2^{args.log2n}, R unique dense keys, S FK Zipf theta={args.theta}",
+            "algo": args.algo, "r_tuples": 1 << args.log2n, "s_tuples": 1 << args.log2n, "theta": args.theta,
+            "tuple": "u32 key + u32 payload", "l2": "inputs 2x larger than L2 (no flush needed)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--algo", default="PRO")
+    ap.add_argument("--log2n", type=int, default=27)
+    ap.add_argument("--theta", type=float, default=0.0)
+    ap.add_argument("--cpu-budget", type=float, default=10.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import torch
+    import alliancedb_b200 as adb
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    n = 1 << args.log2n
+    R, S = make_inputs(adb, n, args.theta, 1 + 1000 * rank)
+    dev = torch.device("cuda", local)
+    dR = torch.from_numpy(R.view(np.int64)).to(dev)
+    dS = torch.from_numpy(S.view(np.int64)).to(dev)
+    hR = torch.from_numpy(R.view(np.int64)).pin_memory()
+    hS = torch.from_numpy(S.view(np.int64)).pin_memory()
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+
+    def step():
+        return adb.join_device(args.algo, dR.data_ptr(), n, dS.data_ptr(), n, None, sp)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    for _ in range(args.warmup):
+        r = step()
+    assert r.count == n, f"FK join must match every S tuple once: {r.count} != {n}"
+    want = (r.count, r.checksum)
+
+    # ---- device-resident timed region
+    phases = []
+    barrier()
+    with ClockSampler(local) as clk:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            r = step()
+            phases.append(r.ms_phase)
+            assert (r.count, r.checksum) == want
+        e1.record(stream)
+        barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    kernels_per_step = r.kernels
+    if dist is not None:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = 2 * n * world / (ms / 1e3)
+
+    # ---- end to end through adb_join with pinned host buffers
+    L = adb.lib()
+    res = adb.JoinResult()
+
+    def step_e2e():
+        st = L.adb_join(args.algo.encode(), hR.data_ptr(), n, hS.data_ptr(), n, None, C.byref(res))
+        if st != 0:
+            raise RuntimeError(L.adb_last_error().decode())
+        return res
+
+    for _ in range(2):
+        step_e2e()
+    barrier()
+    t0 = time.perf_counter()
+    e_ms = []
+    for _ in range(max(1, args.steps // 2)):
+        a = time.perf_counter()
+        rr = step_e2e()
+        e_ms.append((time.perf_counter() - a) * 1e3)
+        assert (rr.count, rr.checksum) == want
+    barrier()
+    e2e_ms = statistics.median(e_ms)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = 2 * n * world / (e2e_ms / 1e3)
+
+    # ---- roofline of the dominant kernel
+    fam = "npo" if args.algo.startswith("NPO") else "radix"
+    ph = np.array(phases).mean(axis=0)
+    cands = PHASE_BYTES[fam]
+    dom = max(cands, key=lambda k: ph[k])
+    kname = {("radix", 1): "part_scatter", ("radix", 3): "radix_join_items", ("radix", 0): "part_hist",
+             ("npo", 0): "npo_build", ("npo", 3): "npo_probe"}[(fam, dom)]
+    hbm, peak_kind = peaks()
+    dom_bytes = cands[dom] * 2 * n
+    achieved = dom_bytes / (ph[dom] / 1e3) / 1e9
+    traffic = load_traffic(kname)
+    pipe_bytes = ALG_BYTES.get(args.algo, 24) * 2 * n
+    pipe_gbs = pipe_bytes / (ms / 1e3) / 1e9
+
+    line = {
+        "metric": "join input tuples/s", "value": value, "unit": "tuples/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32 key/payload (integer)", "data": "synthetic",
+        "config": workload_config(args),
+        "e2e": {"value": e2e_value, "unit": "tuples/s", "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 32,
+                "ms_per_step": e2e_ms},
+        "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "peak_source": peak_kind,
+                     "alg_bytes_per_launch": dom_bytes, "kernel_ms": float(ph[dom]),
+                     "traffic": traffic,
+                     "pipeline": {"alg_bytes_per_tuple": ALG_BYTES.get(args.algo, 24), "achieved": pipe_gbs,
+                                  "frac": pipe_gbs / hbm}},
+        "phases_ms": [float(x) for x in ph],
+        "gpu_launches": kernels_per_step * args.steps,
+        "clocks": clk.summary(),
+        "result": {"count": want[0], "checksum": hex(want[1])},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, reps = cpu_baseline_port(args.algo, 1 << 22, args.cpu_budget)
+        line["cpu_baseline"] = {"value": v, "unit": "tuples/s", "cores": 1, "kind": "port",
+                                "sample": f"oracle {args.algo} restatement on |R|=|S|=2^22 FK, {reps} runs"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()
