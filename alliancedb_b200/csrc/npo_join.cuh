@@ -26,7 +26,8 @@ __host__ __device__ __forceinline__ uint32_t npo_hash(uint32_t key, uint32_t log
     return log2n ? (uint32_t)((key * 0x9E3779B1u) >> (32 - log2n)) : 0u;
 }
 
-__global__ void npo_build(const uint64_t *__restrict__ R, uint64_t nR, uint64_t *__restrict__ table,
+// static: each translation unit that includes this header gets its own copy
+static __global__ void npo_build(const uint64_t *__restrict__ R, uint64_t nR, uint64_t *__restrict__ table,
                           uint32_t log2n, unsigned long long *sentinel_cnt, int *err) {
     const uint64_t mask = (1ULL << log2n) - 1;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;

@@ -172,6 +172,27 @@ int adb_device_sync(void);
 int adb_release_workspace(void);
 
 /* ---------------------------------------------------------------------- */
+/* Allocation-free NPO join.                                              */
+/* ---------------------------------------------------------------------- */
+
+/* No counterpart in the reference: an extra entry point for callers that may
+ * not allocate device memory while they run (an engine that budgets all of
+ * HBM up front, a memory-capped sandbox, a pipeline that must never wait on an
+ * allocator).  It computes exactly what adb_join("NPO", ...) computes, on
+ * device-resident R and S, but its hash table lives in a fixed 32 MiB
+ * __device__ array inside the library instead of allocated memory, so it
+ * calls no cudaMalloc/cudaFree.  Limit: nR <= 2^21 build tuples (larger calls
+ * return ADB_ERR_ARG), nS < 2^32.  d_out is a device array of two uint64:
+ * count, checksum.  Runs on `stream` (a cudaStream_t, NULL = the default
+ * stream) and returns without synchronising.  The first call on each device
+ * looks up the array's device address (cudaGetSymbolAddress) and caches it;
+ * make that first call before any stream capture.  All calls on a device
+ * share the one array: calls that overlap on the GPU race and must be
+ * serialised by the caller. */
+int adb_npo_join_noalloc(const adb_tuple *dR, uint64_t nR, const adb_tuple *dS, uint64_t nS,
+                         uint64_t *d_out, void *stream);
+
+/* ---------------------------------------------------------------------- */
 /* Seeded synthetic relations (the generator of the benchmark configs).   */
 /* Counter-based: element i depends only on (seed, i), so host and device */
 /* produce identical arrays.  Arrays may be host or device pointers as    */
