@@ -194,7 +194,7 @@ static size_t scratch_for(const AlgoEntry *a, uint64_t nR, uint64_t nS, const ad
         case Family::RadixHist:
             return radix_scratch(nR, nS, radix_bits_for(nR, p ? p->radix_bits : 0), num_sms);
         case Family::Npo: return npo_scratch(nR);
-        case Family::SortMerge: return smj_scratch(nR, nS, num_sms);
+        case Family::SortMerge: return smj_scratch(nR, nS, p ? p->part_fanout : 0, num_sms);
         case Family::Shj:
         case Family::Pmj: return eager_scratch(nR, nS, a->fam, eager_batch(p));
         default: return 0;

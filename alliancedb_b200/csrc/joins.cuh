@@ -24,6 +24,14 @@ struct JoinTimes {
 
 enum class Family { Radix, RadixHist, Npo, SortMerge, Shj, Pmj, Unsupported };
 
+// ---- paged partitioning front end (radix and sort-merge joins), paged.cuh ----
+struct PartOut;
+struct DigitFn;
+size_t paged_partition_scratch(uint64_t nR, uint64_t nS, uint32_t b1, uint32_t b2, int num_sms);
+uint64_t paged_final_pool_pages(uint64_t nR, uint64_t nS, uint32_t b1, uint32_t b2, int num_sms);
+int run_paged_partition(Context *ctx, const DevJoin &j, DigitFn d1, const DigitFn *d2, PartOut *out,
+                        unsigned long long *acc);
+
 // ---- radix (PRO / RJ_st / PRH / PRHO) ----
 int radix_bits_for(uint64_t nR, int requested);
 size_t radix_scratch(uint64_t nR, uint64_t nS, int bits, int num_sms);
@@ -34,7 +42,7 @@ size_t npo_scratch(uint64_t nR);
 int run_npo(Context *ctx, const DevJoin &j, unsigned long long *acc);
 
 // ---- m-way / m-pass ----
-size_t smj_scratch(uint64_t nR, uint64_t nS, int num_sms);
+size_t smj_scratch(uint64_t nR, uint64_t nS, int part_fanout, int num_sms);
 int run_smj(Context *ctx, const DevJoin &j, int part_fanout, bool multipass, unsigned long long *acc);
 
 // ---- eager SHJ / PMJ over one window given as arrival-ordered relations ----

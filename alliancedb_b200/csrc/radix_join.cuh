@@ -1,55 +1,127 @@
 // radix_join.cuh -- per-partition build/probe of the partitioned hash joins.
 //
-// Replaces, per partition pair (R_p, S_p) produced by partition.cuh:
+// Replaces, per partition pair (R_p, S_p) produced by paged.cuh:
 //   bucket_chaining_join   hashing/joins/parallel_radix_join.cpp:291-354   (PRO, RJ_st)
 //   histogram_join         hashing/joins/parallel_radix_join.cpp:373-432   (PRH, PRHO)
 // and the task-queue loop of prj_thread (:1409-1416) with a persistent kernel
-// that steals work items from a global counter.  A work item is
-// (partition p, R chunk, S chunk): the R chunk (<= kRCap tuples) is loaded into
-// shared memory with bulk async copies (cp.async.bulk global->shared, completion
-// on an mbarrier), a table is built there, and the S chunk is streamed from
-// global memory and probed.  Partitions whose R side exceeds kRCap (duplicate
-// or skewed build keys) are covered by several R chunks; skewed S partitions
-// by several S chunks, so no item is larger than kRCap x kSChunk.
+// that takes work items from a global counter (work stealing).  A work item is
+// (partition p, R chunk, S chunk): an R chunk is a run of R_p's pages packed
+// greedily up to kRSlots tuples (part_rchunks), copied into shared memory with
+// one bulk async copy per page
+// (cp.async.bulk global->shared, completion counted on an mbarrier), the table
+// is built there, and up to kSPages pages of S_p are streamed from global
+// memory and probed, one warp per page.  Large R partitions (duplicate or
+// skewed build keys, or |R| beyond 2^12 * 16K) take several R chunks; large S
+// partitions (skewed probe keys) several S chunks.
 #pragma once
 
 #include "adb_common.cuh"
-#include "partition.cuh"
+#include "paged.cuh"
 
 namespace adb {
 
 constexpr int kJoinThreads = 1024;
-constexpr uint32_t kRCap = 8192;       // R tuples per item held in shared memory
-constexpr uint32_t kSChunk = 16384;    // S tuples per item
+constexpr uint32_t kRSlots = 17408;                        // R tuples a CTA holds (136 KB)
+constexpr uint32_t kChunkW = kRSlots - kPageTuples;        // chunk weight budget
+constexpr uint32_t kMinPageW = 32;                         // weight floor of a page -> <= 545 pages per chunk
+constexpr uint32_t kRMaxPages = 560;
+constexpr uint32_t kSPages = 1024;                         // S pages per item
+constexpr uint32_t kMaxHeads = 8192;                       // Chain: bucket heads
+constexpr uint32_t kMaxHist = 2048;                        // Hist: buckets
 
-// Work items of a partitioned join: items_off[p] = first item of partition p.
-__global__ void make_items(const uint64_t *starts, uint32_t F, uint32_t *items_off,
-                           uint32_t *n_items, uint32_t rcap, uint32_t schunk) {
+__device__ __forceinline__ uint32_t page_weight(uint32_t cnt) {
+    const uint32_t e = (cnt + 1) & ~1u;                    // slots a page occupies (16-byte copies)
+    return e > kMinPageW ? e : kMinPageW;
+}
+
+// Per partition: R chunk count (greedy by page weight, chunk_w per chunk) and
+// S chunk count (s_pages pages per chunk).  One warp per partition.
+static __global__ void part_rslots(const uint64_t *pstart, const uint32_t *Rlist, const uint8_t *Rcount, uint32_t F,
+                            uint32_t chunk_w, uint32_t s_pages, uint32_t *rch, uint32_t *sch) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t p = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (p >= F) return;
+    const uint64_t *pR = pstart, *pS = pstart + (F + 1);
+    const uint64_t r0 = pR[p], r1 = pR[p + 1];
+    uint64_t wsum = 0, wlast = 0;
+    for (uint64_t k = r0 + lane; k < r1; k += 32) {
+        const uint32_t w = page_weight(Rcount[Rlist[k]]);
+        wsum += w;
+        if (k == r1 - 1) wlast = w;
+    }
+    wsum = warp_sum_u64(wsum);
+    wlast = warp_sum_u64(wlast);
+    if (lane == 0) {
+        const uint64_t nS = pS[p + 1] - pS[p];
+        rch[p] = r1 > r0 ? (uint32_t)((wsum - wlast) / chunk_w + 1) : 0u;
+        sch[p] = (uint32_t)((nS + s_pages - 1) / s_pages);
+    }
+}
+
+// Work items (R chunk x S chunk) and R chunk offsets: items_off[p], chunk_off[p].
+static __global__ void make_items_paged(const uint32_t *rch, const uint32_t *sch, uint32_t F, uint32_t *items_off,
+                                 uint32_t *chunk_off, uint32_t *n_items) {
     __shared__ uint32_t tmp[32];
-    __shared__ uint32_t carry;
-    const uint64_t *sR = starts, *sS = starts + (F + 1);
-    if (threadIdx.x == 0) carry = 0;
+    __shared__ uint32_t carry[2];
+    if (threadIdx.x == 0) carry[0] = carry[1] = 0;
     __syncthreads();
     for (uint32_t base = 0; base < F; base += blockDim.x) {
         const uint32_t p = base + threadIdx.x;
-        uint32_t v = 0;
+        uint32_t vi = 0, vc = 0;
         if (p < F) {
-            const uint64_t nr = sR[p + 1] - sR[p], ns = sS[p + 1] - sS[p];
-            if (nr && ns) v = (uint32_t)(((nr + rcap - 1) / rcap) * ((ns + schunk - 1) / schunk));
+            vc = rch[p];
+            vi = (vc && sch[p]) ? vc * sch[p] : 0u;
         }
-        uint32_t tot;
-        const uint32_t ex = block_exclusive_scan(v, tmp, &tot);
-        if (p < F) items_off[p] = carry + ex;
+        uint32_t ti, tc;
+        const uint32_t ei = block_exclusive_scan(vi, tmp, &ti);
+        const uint32_t ec = block_exclusive_scan(vc, tmp, &tc);
+        if (p < F) {
+            items_off[p] = carry[0] + ei;
+            chunk_off[p] = carry[1] + ec;
+        }
         __syncthreads();
-        if (threadIdx.x == 0) carry += tot;
+        if (threadIdx.x == 0) { carry[0] += ti; carry[1] += tc; }
         __syncthreads();
     }
-    if (threadIdx.x == 0) { items_off[F] = carry; *n_items = carry; }
+    if (threadIdx.x == 0) {
+        items_off[F] = carry[0];
+        chunk_off[F] = carry[1];
+        *n_items = carry[0];
+    }
+}
+
+// First page (page-list index) of every R chunk: chunk c of partition p starts
+// at the first page whose preceding weight in p reaches c * chunk_w.  One warp
+// per partition.
+static __global__ void part_rchunks(const uint64_t *pstart, const uint32_t *Rlist, const uint8_t *Rcount, uint32_t F,
+                             uint32_t chunk_w, const uint32_t *chunk_off, uint64_t *cstart) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t p = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (p >= F) return;
+    const uint64_t r0 = pstart[p], r1 = pstart[p + 1];
+    uint64_t carry = 0;                 // weight before this round
+    uint32_t prev_chunk = 0xFFFFFFFFu;  // chunk of the page before this round
+    for (uint64_t base = r0; base < r1; base += 32) {
+        const uint64_t k = base + lane;
+        const uint32_t w = k < r1 ? page_weight(Rcount[Rlist[k]]) : 0u;
+        uint32_t x = w;                 // inclusive warp scan
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        const uint64_t before = carry + x - w;
+        const uint32_t c = (uint32_t)(before / chunk_w);
+        uint32_t cprev = __shfl_up_sync(0xffffffffu, c, 1);
+        if (lane == 0) cprev = prev_chunk;
+        if (k < r1 && c != cprev) cstart[chunk_off[p] + c] = k;
+        carry += __shfl_sync(0xffffffffu, x, 31);
+        prev_chunk = __shfl_sync(0xffffffffu, c, 31);
+    }
 }
 
 __device__ __forceinline__ uint32_t find_part(const uint32_t *items_off, uint32_t F, uint32_t item) {
-    // largest p with items_off[p] <= item (items_off is non-decreasing)
-    uint32_t lo = 0, hi = F;
+    uint32_t lo = 0, hi = F;   // largest p with items_off[p] <= item
     while (hi - lo > 1) {
         const uint32_t mid = (lo + hi) >> 1;
         if (items_off[mid] <= item) lo = mid; else hi = mid;
@@ -74,7 +146,7 @@ __device__ __forceinline__ void bulk_g2s(void *dst_smem, const void *src_gmem, u
         "l"(src_gmem), "r"(bytes), "r"(b)
         : "memory");
 }
-// Bounded wait on the mbarrier phase; returns false when the bound runs out.
+// Bounded wait on an mbarrier phase; false when the bound runs out.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t phase) {
     const uint32_t a = (uint32_t)__cvta_generic_to_shared(bar);
     for (uint32_t it = 0; it < (1u << 22); it++) {
@@ -91,25 +163,34 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t phase) {
 
 enum class TableKind { Chain = 0, Hist = 1 };
 
-// Shared memory: raw[kRCap + 2] u64 (the R chunk as copied, from the 16-byte
-// boundary at or before its first tuple) | tup2[kRCap] u64 | aux[kRCap] u32 |
-// heads[kRCap + 2] u32 | mbarrier, reduction and item slots.
-constexpr size_t kJoinSmem = ((size_t)kRCap + 2) * 8 + (size_t)kRCap * 8 + (size_t)kRCap * 4 +
-                             ((size_t)kRCap + 2) * 4 + 1024;
+// Shared memory: tup[kRSlots] u64 | aux[kRSlots] u16 | X | pdst[kRMaxPages + 1],
+// pcnt[kRMaxPages + 1] u32 | mbarrier, reduction, item slot and scan scratch.
+// X holds the Chain heads (kMaxHeads u32) or the Hist permutation (kRSlots u16)
+// followed by its bucket starts (kMaxHist + 2 u32).
+constexpr size_t kXBytes = ((size_t)kRSlots * 2 + ((size_t)kMaxHist + 2) * 4) > (size_t)kMaxHeads * 4
+                               ? ((size_t)kRSlots * 2 + ((size_t)kMaxHist + 2) * 4 + 15) & ~(size_t)15
+                               : (size_t)kMaxHeads * 4;
+constexpr size_t kJoinSmem = (size_t)kRSlots * 8 + (size_t)kRSlots * 2 + kXBytes +
+                             ((size_t)kRMaxPages + 1) * 4 * 2 + 1024;
+static_assert(((size_t)kRSlots * 10 + kXBytes + ((size_t)kRMaxPages + 1) * 8) % 8 == 0,
+              "mbarrier must be 8-byte aligned");
+static_assert(kJoinSmem <= 232448, "join kernel exceeds the 227 KB shared-memory limit");
 
 struct JoinArgs {
-    const uint64_t *R;       // partitioned R
-    const uint64_t *S;       // partitioned S
-    const uint64_t *starts;  // [2][F+1]
+    const uint64_t *Rpages, *Spages;
+    const uint8_t *Rcount, *Scount;
+    const uint32_t *Rlist, *Slist;   // page lists grouped by digit
+    const uint64_t *pstart;          // [2][F+1] page-list starts
     const uint32_t *items_off;
+    const uint32_t *chunk_off;       // [F+1] first R chunk of each partition
+    const uint64_t *cstart;          // first page-list index of each R chunk
     const uint32_t *n_items;
     uint32_t *work_counter;
-    unsigned long long *acc;  // [2] count, checksum
-    int *err;                 // set on a timed-out wait
+    unsigned long long *acc;         // [0] count, [1] checksum
+    int *err;
     uint32_t F;
-    uint32_t bits;           // radix bits consumed by the partitioning (hash skips them)
-    // optional materialisation: <S-key, S-payload> per match
-    uint64_t *mat;
+    uint32_t bits;                   // bits the partitioning consumed (the hash skips them)
+    uint64_t *mat;                   // optional <S-key, S-payload> output
     unsigned long long *mat_n;
     uint64_t mat_cap;
 };
@@ -118,13 +199,17 @@ template <TableKind K>
 __global__ void __launch_bounds__(kJoinThreads, 1)
 radix_join_items(JoinArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
-    uint64_t *raw = reinterpret_cast<uint64_t *>(smem);                  // R chunk as copied
-    uint64_t *tup2 = raw + kRCap + 2;                                    // reordered (Hist)
-    uint32_t *aux = reinterpret_cast<uint32_t *>(tup2 + kRCap);          // next[] / ranks
-    uint32_t *heads = aux + kRCap;                                       // bucket heads / hist
-    uint64_t *bar = reinterpret_cast<uint64_t *>(heads + kRCap + 2);
-    uint64_t *red = bar + 2;                                             // 64 u64
-    uint32_t *item_sh = reinterpret_cast<uint32_t *>(red + 64);
+    uint64_t *tup = reinterpret_cast<uint64_t *>(smem);
+    uint16_t *aux = reinterpret_cast<uint16_t *>(tup + kRSlots);        // next[] (Chain) / rank (Hist)
+    unsigned char *xr = reinterpret_cast<unsigned char *>(aux + kRSlots);
+    uint16_t *perm = reinterpret_cast<uint16_t *>(xr);                   // Hist: bucket-ordered slots
+    uint32_t *heads = K == TableKind::Chain ? reinterpret_cast<uint32_t *>(xr)      // Chain: heads
+                                            : reinterpret_cast<uint32_t *>(perm + kRSlots);  // Hist: starts
+    uint32_t *pdst = reinterpret_cast<uint32_t *>(xr + kXBytes);
+    uint32_t *pcnt = pdst + kRMaxPages + 1;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(pcnt + kRMaxPages + 1);
+    uint64_t *red = bar + 2;
+    uint32_t *slots = reinterpret_cast<uint32_t *>(red + 64);            // [0] item, [4..36) scan scratch
 
     const uint32_t n_items = *a.n_items;
     if (threadIdx.x == 0) mbar_init(bar, 1);
@@ -132,128 +217,188 @@ radix_join_items(JoinArgs a) {
     uint32_t phase = 0;
     Acc acc;
     const uint32_t F = a.F;
-    const uint64_t *sR = a.starts, *sS = a.starts + (F + 1);
+    const uint64_t *pR = a.pstart, *pS = a.pstart + (F + 1);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int kWarps = kJoinThreads / 32;
 
     while (true) {
-        if (threadIdx.x == 0) item_sh[0] = atomicAdd(a.work_counter, 1u);
+        if (threadIdx.x == 0) slots[0] = atomicAdd(a.work_counter, 1u);
         __syncthreads();
-        const uint32_t item = item_sh[0];
+        const uint32_t item = slots[0];
         if (item >= n_items) break;
         const uint32_t p = find_part(a.items_off, F, item);
-        const uint64_t r0 = sR[p], nr = sR[p + 1] - r0;
-        const uint64_t s0 = sS[p], ns = sS[p + 1] - s0;
-        const uint32_t sch = (uint32_t)((ns + kSChunk - 1) / kSChunk);
+        const uint64_t r0 = pR[p], nrp = pR[p + 1] - r0;
+        const uint64_t s0 = pS[p], nsp = pS[p + 1] - s0;
+        const uint32_t sch = (uint32_t)((nsp + kSPages - 1) / kSPages);
         const uint32_t local = item - a.items_off[p];
         const uint32_t rc = local / sch, sc = local % sch;
-        const uint64_t rb = r0 + (uint64_t)rc * kRCap;
-        const uint32_t nrc = (uint32_t)min((uint64_t)kRCap, nr - (uint64_t)rc * kRCap);
-        const uint64_t sb = s0 + (uint64_t)sc * kSChunk;
-        const uint32_t nsc = (uint32_t)min((uint64_t)kSChunk, ns - (uint64_t)sc * kSChunk);
+        const uint32_t cid = a.chunk_off[p] + rc;
+        const uint64_t rb = a.cstart[cid];
+        const uint64_t re = rc + 1 < a.chunk_off[p + 1] - a.chunk_off[p] ? a.cstart[cid + 1] : r0 + nrp;
+        const uint32_t nrpg = (uint32_t)(re - rb);
+        const uint64_t sb = s0 + (uint64_t)sc * kSPages;
+        const uint32_t nspg = (uint32_t)min((uint64_t)kSPages, nsp - (uint64_t)sc * kSPages);
 
-        // --- load the R chunk with one bulk async copy.  The copy starts at the
-        //     16-byte boundary at or before the chunk (o = 0 or 1 tuple early)
-        //     and is rounded up to 16 bytes; the partition buffers carry two
-        //     tuples of slack so both ends stay inside the allocation.
-        const uint64_t *src = a.R + rb;
-        const uint32_t o = (uint32_t)((reinterpret_cast<uintptr_t>(src) & 15) >> 3);
-        const uint32_t copy_bytes = ((o + nrc) * 8 + 15) & ~15u;
-        const uint64_t *tup = raw + o;
+        // --- R chunk: page counts, 16-byte aligned destinations, one bulk copy per page
+        uint32_t tot_slots = 0;
+        for (uint32_t base = 0; base < nrpg; base += blockDim.x) {
+            const uint32_t k = base + threadIdx.x;
+            uint32_t pg = 0, cnt = 0;
+            if (k < nrpg) {
+                pg = a.Rlist[rb + k];
+                cnt = a.Rcount[pg];
+            }
+            uint32_t tot;
+            const uint32_t dst = tot_slots + block_exclusive_scan((cnt + 1) & ~1u, slots + 4, &tot);
+            if (k < nrpg) {
+                pdst[k] = dst;
+                pcnt[k] = cnt;
+            }
+            tot_slots += tot;
+        }
         if (threadIdx.x == 0) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            mbar_expect_tx(bar, copy_bytes);
-            bulk_g2s(raw, src - o, copy_bytes, bar);
+            mbar_expect_tx(bar, tot_slots * 8);
         }
-        uint32_t nb;   // buckets
+        __syncthreads();
+        for (uint32_t k = threadIdx.x; k < nrpg; k += blockDim.x) {
+            const uint32_t cnt = pcnt[k];
+            if (cnt) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                bulk_g2s(tup + pdst[k], a.Rpages + (uint64_t)a.Rlist[rb + k] * kPageTuples, ((cnt + 1) & ~1u) * 8,
+                         bar);
+            }
+        }
+
+        uint32_t nb = 1;
+        while (nb < tot_slots) nb <<= 1;
         if (K == TableKind::Chain) {
-            nb = 1;
-            while (nb < nrc) nb <<= 1;                      // NEXT_POW_2(|R_i|)
+            nb >>= 1;                                  // about two slots per head
+            if (nb > kMaxHeads) nb = kMaxHeads;
         } else {
-            nb = 1;
-            while (nb < nrc) nb <<= 1;
-            nb >>= 2;
-            if (nb < 4) nb = 4;                             // get_hist_size
+            nb >>= 2;                                  // get_hist_size: |R_i| / 4 buckets
+            if (nb > kMaxHist) nb = kMaxHist;
         }
+        if (nb < 1) nb = 1;
         const uint32_t bmask = nb - 1;
         for (uint32_t i = threadIdx.x; i < nb + 2; i += blockDim.x) heads[i] = 0;
         if (!mbar_wait(bar, phase)) atomicExch(a.err, 1);
         phase ^= 1;
         __syncthreads();
 
+        // --- build (warp per page, two tuples per lane)
         if (K == TableKind::Chain) {
-            // build: next[i] = bucket[idx]; bucket[idx] = i + 1
-            for (uint32_t i = threadIdx.x; i < nrc; i += blockDim.x) {
-                const uint32_t h = (tkey(tup[i]) >> a.bits) & bmask;
-                aux[i] = atomicExch(&heads[h], i + 1);
+            for (uint32_t k = warp; k < nrpg; k += kWarps) {
+                const uint32_t c = pcnt[k], base = pdst[k];
+                for (uint32_t l = lane; l < c; l += 32) {
+                    const uint32_t s = base + l;
+                    const uint32_t h = (tkey(tup[s]) >> a.bits) & bmask;
+                    aux[s] = (uint16_t)atomicExch(&heads[h], s + 1);
+                }
             }
             __syncthreads();
         } else {
-            // histogram + prefix + reorder into tup2 (bucket-contiguous)
-            for (uint32_t i = threadIdx.x; i < nrc; i += blockDim.x) {
-                const uint32_t h = (tkey(tup[i]) >> a.bits) & bmask;
-                aux[i] = atomicAdd(&heads[h + 1], 1u);
+            for (uint32_t k = warp; k < nrpg; k += kWarps) {
+                const uint32_t c = pcnt[k], base = pdst[k];
+                for (uint32_t l = lane; l < c; l += 32) {
+                    const uint32_t s = base + l;
+                    const uint32_t h = (tkey(tup[s]) >> a.bits) & bmask;
+                    aux[s] = (uint16_t)atomicAdd(&heads[h + 1], 1u);
+                }
             }
             __syncthreads();
-            {
+            {   // bucket starts: heads[h + 1] = start of bucket h, heads[nb + 1] = total
                 const uint32_t per = (nb + blockDim.x - 1) / blockDim.x;
-                const uint32_t d0 = threadIdx.x * per;
+                const uint32_t d0 = threadIdx.x * per, d1 = min(nb, d0 + per);
                 uint32_t loc = 0;
-                for (uint32_t d = d0; d < min(nb, d0 + per); d++) loc += heads[d + 1];
+                for (uint32_t d = d0; d < d1; d++) loc += heads[d + 1];
                 uint32_t tot;
-                uint32_t ex = block_exclusive_scan(loc, item_sh + 4, &tot);
-                __syncthreads();
-                for (uint32_t d = d0; d < min(nb, d0 + per); d++) {
+                uint32_t ex = block_exclusive_scan(loc, slots + 4, &tot);
+                for (uint32_t d = d0; d < d1; d++) {
                     const uint32_t c = heads[d + 1];
-                    heads[d + 1] = ex;     // heads[h+1] = start of bucket h
+                    heads[d + 1] = ex;
                     ex += c;
                 }
+                __syncthreads();
                 if (threadIdx.x == 0) heads[nb + 1] = tot;
             }
             __syncthreads();
-            for (uint32_t i = threadIdx.x; i < nrc; i += blockDim.x) {
-                const uint32_t h = (tkey(tup[i]) >> a.bits) & bmask;
-                tup2[heads[h + 1] + aux[i]] = tup[i];
+            for (uint32_t k = warp; k < nrpg; k += kWarps) {
+                const uint32_t c = pcnt[k], base = pdst[k];
+                for (uint32_t l = lane; l < c; l += 32) {
+                    const uint32_t s = base + l;
+                    const uint32_t h = (tkey(tup[s]) >> a.bits) & bmask;
+                    perm[heads[h + 1] + aux[s]] = (uint16_t)s;
+                }
             }
             __syncthreads();
         }
 
-        // --- probe the S chunk
-        const uint64_t *S = a.S + sb;
-        for (uint32_t j = threadIdx.x; j < nsc; j += blockDim.x) {
-            const uint64_t s = ld_stream(S + j);
-            const uint32_t key = tkey(s);
-            const uint32_t h = (key >> a.bits) & bmask;
-            uint64_t sh = 0;
-            bool have_sh = false;
-            if (K == TableKind::Chain) {
-                for (uint32_t hit = heads[h]; hit; hit = aux[hit - 1]) {
-                    const uint64_t r = tup[hit - 1];
-                    if (tkey(r) == key) {
-                        if (!have_sh) { sh = s_half(key, tpay(s)); have_sh = true; }
-                        acc.count++;
-                        acc.sum += pair_hash_pre(key, tpay(r), sh);
-                        if (a.mat) {
-                            const unsigned long long slot = atomicAdd(a.mat_n, 1ull);
-                            if (slot < a.mat_cap) a.mat[slot] = s;
+        // --- probe the S chunk.  Warp w takes pages w, w + 32, ...: lane i holds
+        //     the id and count of the warp's i-th page, and the tuples of the
+        //     next page are loaded before the current page is probed.
+        {
+            const uint32_t npw = warp < (int)nspg ? (nspg - warp + kWarps - 1) / kWarps : 0;
+            uint32_t my_pg = 0, my_cnt = 0;
+            if (lane < (int)npw) {
+                my_pg = a.Slist[sb + warp + (uint64_t)kWarps * lane];
+                my_cnt = a.Scount[my_pg];
+            }
+            uint64_t c0 = 0, c1 = 0;
+            uint32_t ccnt = 0;
+            auto load_page = [&](uint32_t i, uint64_t &x0, uint64_t &x1, uint32_t &cn) {
+                const uint32_t pgi = __shfl_sync(0xffffffffu, my_pg, i);
+                cn = __shfl_sync(0xffffffffu, my_cnt, i);
+                const uint64_t *Sp = a.Spages + (uint64_t)pgi * kPageTuples;
+                x0 = lane < (int)cn ? ld_stream(Sp + lane) : 0;
+                x1 = lane + 32 < (int)cn ? ld_stream(Sp + lane + 32) : 0;
+            };
+            if (npw) load_page(0, c0, c1, ccnt);
+            for (uint32_t i = 0; i < npw; i++) {
+                uint64_t n0 = 0, n1 = 0;
+                uint32_t ncnt = 0;
+                if (i + 1 < npw) load_page(i + 1, n0, n1, ncnt);
+#pragma unroll
+                for (int half = 0; half < 2; half++) {
+                    if (lane + 32 * half >= (int)ccnt) continue;
+                    const uint64_t s = half ? c1 : c0;
+                    const uint32_t key = tkey(s);
+                    const uint32_t h = (key >> a.bits) & bmask;
+                    uint64_t sh = 0;
+                    bool have_sh = false;
+                    if (K == TableKind::Chain) {
+                        for (uint32_t hit = heads[h]; hit; hit = aux[hit - 1]) {
+                            const uint64_t r = tup[hit - 1];
+                            if (tkey(r) == key) {
+                                if (!have_sh) { sh = s_half(key, tpay(s)); have_sh = true; }
+                                acc.count++;
+                                acc.sum += pair_hash_pre(key, tpay(r), sh);
+                                if (a.mat) {
+                                    const unsigned long long m = atomicAdd(a.mat_n, 1ull);
+                                    if (m < a.mat_cap) a.mat[m] = s;
+                                }
+                            }
+                        }
+                    } else {
+                        const uint32_t e = heads[h + 2];
+                        for (uint32_t t = heads[h + 1]; t < e; t++) {
+                            const uint64_t r = tup[perm[t]];
+                            if (tkey(r) == key) {
+                                if (!have_sh) { sh = s_half(key, tpay(s)); have_sh = true; }
+                                acc.count++;
+                                acc.sum += pair_hash_pre(key, tpay(r), sh);
+                                if (a.mat) {
+                                    const unsigned long long m = atomicAdd(a.mat_n, 1ull);
+                                    if (m < a.mat_cap) a.mat[m] = s;
+                                }
+                            }
                         }
                     }
                 }
-            } else {
-                const uint32_t e = heads[h + 2];
-                for (uint32_t t = heads[h + 1]; t < e; t++) {
-                    const uint64_t r = tup2[t];
-                    if (tkey(r) == key) {
-                        if (!have_sh) { sh = s_half(key, tpay(s)); have_sh = true; }
-                        acc.count++;
-                        acc.sum += pair_hash_pre(key, tpay(r), sh);
-                        if (a.mat) {
-                            const unsigned long long slot = atomicAdd(a.mat_n, 1ull);
-                            if (slot < a.mat_cap) a.mat[slot] = s;
-                        }
-                    }
-                }
+                c0 = n0; c1 = n1; ccnt = ncnt;
             }
         }
-        __syncthreads();   // table is rebuilt by the next item
+        __syncthreads();   // the next item rebuilds the table
     }
     block_flush(acc, a.acc, red);
 }

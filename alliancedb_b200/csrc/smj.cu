@@ -1,11 +1,382 @@
 // smj.cu -- sort-merge joins (m-way, m-pass, m-way+skew).
+//
+// Reference: sortmergejoin_multiway (sorting/joins/sortmergejoin_multiway.cpp:55-700):
+// partitioning_phase (MSB radix into PARTFANOUT partitions, :435-497),
+// sorting_phase (AVX sort of each partition, :499-567), multiwaymerge_phase
+// (:569-660) and mergejoin_phase -> merge_join (sorting/joins/common_functions.cpp
+// :298-372), which joins two sorted runs including the cross product of
+// duplicate keys.  m-pass (sortmergejoin_multipass.cpp) differs only in merging
+// pairwise.
+//
+// On the device both names run one pipeline:
+//   1. the paged partitioning front end (radix.cu) on the low key bits: equal
+//      keys meet in one partition, as the reference's range partition
+//      guarantees for its key ranges;
+//   2. smj_items, a persistent work-stealing kernel: per work item it copies an
+//      R chunk (<= 8192 tuples) into shared memory with bulk async copies, sorts
+//      it, loads and sorts the item's S block, and merge-joins the two sorted
+//      runs with merge-path partitioning across the CTA's threads.
+// The per-chunk sort is an MSD counting sort on the (at most) 12 highest key
+// bits that differ within the chunk, followed by an insertion sort inside
+// each bucket: the bits above those are equal across the chunk, so the result
+// is fully sorted by key.  Ties between equal keys stay in arbitrary order,
+// which merge_join does not depend on.
 #include "joins.cuh"
+#include "paged.cuh"
+#include "radix_join.cuh"
 
 namespace adb {
-size_t smj_scratch(uint64_t, uint64_t, int) { return 0; }
-int run_smj(Context *, const DevJoin &, int, bool, unsigned long long *) {
-    set_error("m-way is not built yet");
-    return ADB_ERR_UNSUPPORTED;
+
+constexpr uint32_t kSmjCap = 8192;                  // tuples per R chunk and per S block
+constexpr uint32_t kSmjChunkW = kSmjCap - kPageTuples;
+constexpr uint32_t kSmjSPages = kSmjCap / kPageTuples;   // 128 pages <= 8192 tuples
+constexpr uint32_t kSmjMaxPages = 272;              // weight floor 32: <= 8192 / 32 + 1 pages per chunk
+constexpr uint32_t kSmjBucketBits = 12;
+constexpr uint32_t kSmjThreads = 1024;
+
+// A | B | C tuple buffers, bucket counters, R page table, barrier and scratch.
+constexpr size_t kSmjSmem = (size_t)kSmjCap * 8 * 3 + ((size_t)(1u << kSmjBucketBits) + 4) * 4 +
+                            ((size_t)kSmjMaxPages + 1) * 4 * 2 + 1024;
+static_assert(kSmjSmem <= 232448, "smj_items exceeds the 227 KB shared-memory limit");
+
+struct SmjArgs {
+    const uint64_t *Rpages, *Spages;
+    const uint8_t *Rcount, *Scount;
+    const uint32_t *Rlist, *Slist;
+    const uint64_t *pstart;          // [2][F+1]
+    const uint32_t *items_off, *chunk_off;
+    const uint64_t *cstart;
+    const uint32_t *n_items;
+    uint32_t *work_counter;
+    unsigned long long *acc;
+    int *err;
+    uint32_t F;
+    uint64_t *mat;
+    unsigned long long *mat_n;
+    uint64_t mat_cap;
+};
+
+// Sorts src[0..n) by key into dst (both shared memory).  cnt holds 2^12 + 1
+// counters; red holds 64 scratch words.  All threads call it.
+__device__ void chunk_sort(const uint64_t *src, uint32_t n, uint64_t *dst, uint32_t *cnt, uint32_t *red) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    // key bits that differ within the chunk
+    uint32_t a = 0xFFFFFFFFu, o = 0;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const uint32_t k = tkey(src[i]);
+        a &= k;
+        o |= k;
+    }
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) {
+        a &= __shfl_xor_sync(0xffffffffu, a, s);
+        o |= __shfl_xor_sync(0xffffffffu, o, s);
+    }
+    if (lane == 0) { red[wid] = a; red[32 + wid] = o; }
+    __syncthreads();
+    a = 0xFFFFFFFFu;
+    o = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) { a &= red[w]; o |= red[32 + w]; }
+    const uint32_t vary = a ^ o;
+    __syncthreads();
+    if (vary == 0) {   // one key value: already sorted
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+        __syncthreads();
+        return;
+    }
+    const uint32_t hi = 31 - __clz(vary);
+    const uint32_t nbits = hi + 1 < kSmjBucketBits ? hi + 1 : kSmjBucketBits;
+    const uint32_t shift = hi + 1 - nbits;
+    const uint32_t nb = 1u << nbits, bmask = nb - 1;
+    for (uint32_t d = threadIdx.x; d < nb; d += blockDim.x) cnt[d] = 0;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) atomicAdd(&cnt[(tkey(src[i]) >> shift) & bmask], 1u);
+    __syncthreads();
+    {   // exclusive scan of the bucket counts, contiguous buckets per thread
+        const uint32_t per = (nb + blockDim.x - 1) / blockDim.x;
+        const uint32_t d0 = threadIdx.x * per, d1 = min(nb, d0 + per);
+        uint32_t loc = 0;
+        for (uint32_t d = d0; d < d1; d++) loc += cnt[d];
+        uint32_t tot;
+        uint32_t ex = block_exclusive_scan(loc, red, &tot);
+        for (uint32_t d = d0; d < d1; d++) {
+            const uint32_t c = cnt[d];
+            cnt[d] = ex;
+            ex += c;
+        }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const uint64_t v = src[i];
+        dst[atomicAdd(&cnt[(tkey(v) >> shift) & bmask], 1u)] = v;
+    }
+    __syncthreads();
+    // cnt[d] is now the end of bucket d.  Buckets of more than 128 tuples
+    // (keys clustered below the bucket bits) would make the insertion sort
+    // quadratic: then the whole chunk is bitonic-sorted on the 64-bit word
+    // instead, padded with all-ones words that sort last.
+    if (shift) {
+        int big = 0;
+        for (uint32_t d = threadIdx.x; d < nb; d += blockDim.x)
+            if (cnt[d] - (d ? cnt[d - 1] : 0u) > 128) big = 1;
+        if (__syncthreads_or(big)) {
+            uint32_t m = 1;
+            while (m < n) m <<= 1;
+            for (uint32_t i = n + threadIdx.x; i < m; i += blockDim.x) dst[i] = ~0ULL;
+            __syncthreads();
+            for (uint32_t k = 2; k <= m; k <<= 1) {
+                for (uint32_t jj = k >> 1; jj > 0; jj >>= 1) {
+                    for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+                        const uint32_t l = i ^ jj;
+                        if (l > i) {
+                            const uint64_t x = dst[i], y = dst[l];
+                            const bool up = (i & k) == 0;
+                            if ((x > y) == up) { dst[i] = y; dst[l] = x; }
+                        }
+                    }
+                    __syncthreads();
+                }
+            }
+            return;
+        }
+        for (uint32_t d = threadIdx.x; d < nb; d += blockDim.x) {
+            const uint32_t b = d ? cnt[d - 1] : 0u, e = cnt[d];
+            for (uint32_t i = b + 1; i < e; i++) {
+                const uint64_t v = dst[i];
+                const uint32_t k = tkey(v);
+                uint32_t j = i;
+                while (j > b && tkey(dst[j - 1]) > k) {
+                    dst[j] = dst[j - 1];
+                    j--;
+                }
+                dst[j] = v;
+            }
+        }
+        __syncthreads();
+    }
 }
-int smj_set_attrs() { return ADB_OK; }
+
+__global__ void __launch_bounds__(kSmjThreads, 1)
+smj_items(SmjArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint64_t *A = reinterpret_cast<uint64_t *>(smem);       // sorted R chunk (bulk-copy target first)
+    uint64_t *B = A + kSmjCap;                              // compact staging
+    uint64_t *C = B + kSmjCap;                              // sorted S block
+    uint32_t *cnt = reinterpret_cast<uint32_t *>(C + kSmjCap);
+    uint32_t *pdst = cnt + (1u << kSmjBucketBits) + 4;
+    uint32_t *pcnt = pdst + kSmjMaxPages + 1;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(pcnt + kSmjMaxPages + 1);
+    uint64_t *red = bar + 2;                                 // 64 u64
+    uint32_t *slots = reinterpret_cast<uint32_t *>(red + 64);
+
+    const uint32_t n_items = *a.n_items;
+    if (threadIdx.x == 0) mbar_init(bar, 1);
+    __syncthreads();
+    uint32_t phase = 0;
+    Acc acc;
+    const uint32_t F = a.F;
+    const uint64_t *pR = a.pstart, *pS = a.pstart + (F + 1);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int kWarps = kSmjThreads / 32;
+
+    while (true) {
+        if (threadIdx.x == 0) slots[0] = atomicAdd(a.work_counter, 1u);
+        __syncthreads();
+        const uint32_t item = slots[0];
+        if (item >= n_items) break;
+        const uint32_t p = find_part(a.items_off, F, item);
+        const uint64_t r0 = pR[p], nrp = pR[p + 1] - r0;
+        const uint64_t s0 = pS[p], nsp = pS[p + 1] - s0;
+        const uint32_t sch = (uint32_t)((nsp + kSmjSPages - 1) / kSmjSPages);
+        const uint32_t local = item - a.items_off[p];
+        const uint32_t rc = local / sch, sc = local % sch;
+        const uint32_t cid = a.chunk_off[p] + rc;
+        const uint64_t rb = a.cstart[cid];
+        const uint64_t re = rc + 1 < a.chunk_off[p + 1] - a.chunk_off[p] ? a.cstart[cid + 1] : r0 + nrp;
+        const uint32_t nrpg = (uint32_t)(re - rb);
+        const uint64_t sb = s0 + (uint64_t)sc * kSmjSPages;
+        const uint32_t nspg = (uint32_t)min((uint64_t)kSmjSPages, nsp - (uint64_t)sc * kSmjSPages);
+
+        // --- R chunk -> A (bulk copies, 16-byte aligned slots per page)
+        uint32_t tot_slots = 0, nr = 0;
+        for (uint32_t base = 0; base < nrpg; base += blockDim.x) {
+            const uint32_t k = base + threadIdx.x;
+            uint32_t cnt_k = 0;
+            if (k < nrpg) cnt_k = a.Rcount[a.Rlist[rb + k]];
+            uint32_t tot;
+            const uint32_t dst = tot_slots + block_exclusive_scan((cnt_k + 1) & ~1u, slots + 4, &tot);
+            if (k < nrpg) { pdst[k] = dst; pcnt[k] = cnt_k; }
+            tot_slots += tot;
+        }
+        if (threadIdx.x == 0) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_expect_tx(bar, tot_slots * 8);
+        }
+        __syncthreads();
+        for (uint32_t k = threadIdx.x; k < nrpg; k += blockDim.x) {
+            const uint32_t c = pcnt[k];
+            if (c) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                bulk_g2s(A + pdst[k], a.Rpages + (uint64_t)a.Rlist[rb + k] * kPageTuples, ((c + 1) & ~1u) * 8, bar);
+            }
+        }
+        // --- S block -> C (compact, plain loads), overlapping the R copies
+        {
+            uint32_t soff = 0;
+            for (uint32_t base = 0; base < nspg; base += blockDim.x) {
+                const uint32_t k = base + threadIdx.x;
+                uint32_t c = 0;
+                if (k < nspg) c = a.Scount[a.Slist[sb + k]];
+                uint32_t tot;
+                const uint32_t off = soff + block_exclusive_scan(c, slots + 4, &tot);
+                if (k < nspg) cnt[k] = off;            // page offsets (cnt is free until the sorts)
+                soff += tot;
+            }
+            __syncthreads();
+            for (uint32_t k = warp; k < nspg; k += kWarps) {
+                const uint32_t pg = a.Slist[sb + k];
+                const uint32_t c = a.Scount[pg];
+                const uint32_t off = cnt[k];
+                const uint64_t *src = a.Spages + (uint64_t)pg * kPageTuples;
+                for (uint32_t l = lane; l < c; l += 32) C[off + l] = ld_stream(src + l);
+            }
+            if (threadIdx.x == 0) slots[1] = soff;
+        }
+        if (!mbar_wait(bar, phase)) atomicExch(a.err, 1);
+        phase ^= 1;
+        __syncthreads();
+        const uint32_t ns = slots[1];
+        // compact R: A (page slots) -> B
+        {
+            uint32_t roff = 0;
+            for (uint32_t base = 0; base < nrpg; base += blockDim.x) {
+                const uint32_t k = base + threadIdx.x;
+                const uint32_t c = k < nrpg ? pcnt[k] : 0u;
+                uint32_t tot;
+                const uint32_t off = roff + block_exclusive_scan(c, slots + 4, &tot);
+                if (k < nrpg) cnt[k] = off;
+                roff += tot;
+            }
+            nr = roff;
+            __syncthreads();
+            for (uint32_t k = warp; k < nrpg; k += kWarps) {
+                const uint32_t c = pcnt[k], src = pdst[k], dst = cnt[k];
+                for (uint32_t l = lane; l < c; l += 32) B[dst + l] = A[src + l];
+            }
+            __syncthreads();
+        }
+        chunk_sort(B, nr, A, cnt, reinterpret_cast<uint32_t *>(red));   // sorted R in A
+        chunk_sort(C, ns, B, cnt, reinterpret_cast<uint32_t *>(red));   // sorted S in B
+
+        // --- merge-path join of A (R, nr) and B (S, ns); R first on equal keys
+        {
+            const uint32_t total = nr + ns;
+            const uint32_t L = (total + blockDim.x - 1) / blockDim.x;
+            const uint32_t k0 = min(total, threadIdx.x * L), k1 = min(total, k0 + L);
+            uint32_t lo = k0 > ns ? k0 - ns : 0u, hi = k0 < nr ? k0 : nr;
+            while (lo < hi) {   // number of R tuples among the first k0 merged
+                const uint32_t mid = (lo + hi) >> 1;
+                if (tkey(A[mid]) <= tkey(B[k0 - mid - 1])) lo = mid + 1; else hi = mid;
+            }
+            uint32_t i = lo, j = k0 - lo;
+            for (uint32_t k = k0; k < k1; k++) {
+                if (j >= ns || (i < nr && tkey(A[i]) <= tkey(B[j]))) {
+                    i++;
+                } else {
+                    const uint64_t s = B[j];
+                    const uint32_t key = tkey(s);
+                    uint64_t sh = 0;
+                    bool have = false;
+                    for (int t = (int)i - 1; t >= 0 && tkey(A[t]) == key; t--) {
+                        if (!have) { sh = s_half(key, tpay(s)); have = true; }
+                        acc.count++;
+                        acc.sum += pair_hash_pre(key, tpay(A[t]), sh);
+                        if (a.mat) {
+                            const unsigned long long m = atomicAdd(a.mat_n, 1ull);
+                            if (m < a.mat_cap) a.mat[m] = s;
+                        }
+                    }
+                    j++;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    block_flush(acc, a.acc, red);
+}
+
+static void smj_bits(uint64_t nR, int part_fanout, uint32_t *b1, uint32_t *b2) {
+    int bits;
+    if (part_fanout > 1) {
+        bits = (int)ceil_log2_u64((uint64_t)part_fanout);
+    } else {
+        bits = (int)ceil_log2_u64((nR + 4095) / 4096);   // R partitions of about half a chunk
+    }
+    if (bits < 1) bits = 1;
+    if (bits > 16) bits = 16;
+    if (bits <= (int)kSmallPassBits) {
+        *b1 = bits;
+        *b2 = 0;
+    } else {
+        *b1 = bits / 2;
+        *b2 = bits - bits / 2;
+    }
+}
+
+size_t smj_scratch(uint64_t nR, uint64_t nS, int part_fanout, int num_sms) {
+    uint32_t b1, b2;
+    smj_bits(nR, part_fanout, &b1, &b2);
+    const uint64_t F = 1ull << (b1 + b2);
+    const uint64_t pages = paged_final_pool_pages(nR, nS, b1, b2, num_sms);
+    return paged_partition_scratch(nR, nS, b1, b2, num_sms) + Workspace::need(F, 4) * 2 +
+           Workspace::need(F + 1, 4) * 2 + Workspace::need(pages * kPageTuples / kSmjChunkW + F + 1, 8) +
+           Workspace::need(2, 4);
+}
+
+int run_smj(Context *ctx, const DevJoin &j, int part_fanout, bool /*multipass*/, unsigned long long *acc) {
+    cudaStream_t st = ctx->stream;
+    uint32_t b1, b2;
+    smj_bits(j.nR, part_fanout, &b1, &b2);
+    const DigitFn d1{0u, 0u, (1u << b1) - 1};
+    const DigitFn d2{0u, b1, (1u << b2) - 1};
+    PartOut po;
+    ADB_TRY(run_paged_partition(ctx, j, d1, b2 ? &d2 : nullptr, &po, acc));
+    ADB_CK(cudaEventRecord(ctx->ev[1], st));
+
+    const uint32_t F = po.Fout;
+    uint32_t *rch = ctx->ws.take<uint32_t>(F);
+    uint32_t *sch = ctx->ws.take<uint32_t>(F);
+    uint32_t *items_off = ctx->ws.take<uint32_t>(F + 1);
+    uint32_t *chunk_off = ctx->ws.take<uint32_t>(F + 1);
+    uint64_t *cstart = ctx->ws.take<uint64_t>(po.pool_pages * kPageTuples / kSmjChunkW + F + 1);
+    uint32_t *ctr = ctx->ws.take<uint32_t>(2);
+    ADB_CK(cudaMemsetAsync(ctr, 0, 2 * sizeof(uint32_t), st));
+    part_rslots<<<(F + 7) / 8, 256, 0, st>>>(po.pstart, po.R.plist, po.R.pcount, F, kSmjChunkW, kSmjSPages, rch,
+                                             sch);
+    make_items_paged<<<1, 1024, 0, st>>>(rch, sch, F, items_off, chunk_off, ctr);
+    part_rchunks<<<(F + 7) / 8, 256, 0, st>>>(po.pstart, po.R.plist, po.R.pcount, F, kSmjChunkW, chunk_off, cstart);
+    ADB_CK(cudaGetLastError());
+    ADB_CK(cudaEventRecord(ctx->ev[2], st));
+    ADB_CK(cudaEventRecord(ctx->ev[3], st));
+
+    SmjArgs a;
+    a.Rpages = po.R.pages; a.Spages = po.S.pages;
+    a.Rcount = po.R.pcount; a.Scount = po.S.pcount;
+    a.Rlist = po.R.plist; a.Slist = po.S.plist;
+    a.pstart = po.pstart; a.items_off = items_off; a.chunk_off = chunk_off; a.cstart = cstart;
+    a.n_items = ctr; a.work_counter = ctr + 1;
+    a.acc = acc; a.err = reinterpret_cast<int *>(acc + 2);
+    a.F = F;
+    a.mat = j.mat; a.mat_n = acc + 3; a.mat_cap = j.mat_cap;
+    smj_items<<<ctx->num_sms, kSmjThreads, kSmjSmem, st>>>(a);
+    ADB_CK(cudaGetLastError());
+    ctx->kernels += 4;
+    return ADB_OK;
+}
+
+int smj_set_attrs() {
+    ADB_CK(cudaFuncSetAttribute(smj_items, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmjSmem));
+    return ADB_OK;
+}
+
 }  // namespace adb

@@ -46,7 +46,7 @@ sys.path.insert(0, str(ROOT))
 ALG_BYTES = {"PRO": 24, "RJ_st": 24, "PRH": 24, "PRHO": 24, "NPO": 16, "NPO_st": 16,
              "m-way": 24, "m-pass": 24, "m-way+skew": 24}
 # dominant-phase index and its algorithmic bytes per input tuple
-PHASE_BYTES = {"radix": {1: 16, 3: 8, 0: 8}, "npo": {0: 8, 3: 8}}
+PHASE_BYTES = {"radix": {0: 16, 3: 8}, "npo": {0: 8, 3: 8}}
 
 
 def peaks():
@@ -291,7 +291,7 @@ def main():
     ph = np.array(phases).mean(axis=0)
     cands = PHASE_BYTES[fam]
     dom = max(cands, key=lambda k: ph[k])
-    kname = {("radix", 1): "part_scatter", ("radix", 3): "radix_join_items", ("radix", 0): "part_hist",
+    kname = {("radix", 0): "paged_scatter", ("radix", 3): "radix_join_items",
              ("npo", 0): "npo_build", ("npo", 3): "npo_probe"}[(fam, dom)]
     hbm, peak_kind = peaks()
     dom_bytes = cands[dom] * 2 * n

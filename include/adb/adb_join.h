@@ -88,7 +88,7 @@ typedef struct adb_join_result {
     int32_t status;             /* adb_status */
     int32_t kernels;            /* kernels this call launched */
     float ms_device;            /* device time of the join, CUDA events on the library stream */
-    float ms_phase[4];          /* device time per phase; radix: histograms, scatter, work list, join kernel;
+    float ms_phase[4];          /* device time per phase; radix: scatter, page lists + work list, -, join kernel;
                                    NPO: build, -, -, probe */
     float ms_h2d;               /* host->device copy time (adb_join only) */
     uint64_t materialized;      /* tuples written to the materialisation buffer */

@@ -12,7 +12,7 @@ import alliancedb_b200 as adb
 
 pytestmark = pytest.mark.gpu
 
-LAZY = ["PRO", "RJ_st", "PRH", "PRHO", "NPO", "NPO_st"]
+LAZY = ["PRO", "RJ_st", "PRH", "PRHO", "NPO", "NPO_st", "m-way", "m-pass", "m-way+skew"]
 
 
 def fk_pair(n_r, n_s, theta=0.0, seed=7):
@@ -83,6 +83,22 @@ def test_empty(oracle, algo):
 def test_radix_bits(oracle, algo, bits):
     R, S = fk_pair(50000, 70001, 0.8)
     check(oracle, algo, R, S, radix_bits=bits)
+
+
+@pytest.mark.parametrize("fanout", [2, 64, 1 << 12, 1 << 16])
+def test_smj_part_fanout(oracle, fanout):
+    """joinconfig_t.PARTFANOUT (sorting/utils/types.h:117-124) changes the plan, not the result."""
+    R, S = fk_pair(40000, 50001, 1.2)
+    check(oracle, "m-way", R, S, part_fanout=fanout)
+
+
+@pytest.mark.parametrize("algo", ["m-way", "PRO"])
+def test_clustered_keys_with_outlier(oracle, algo):
+    """Dense small keys plus one far key: one sort bucket would hold nearly all tuples."""
+    keys = np.concatenate([np.arange(1, 60001, dtype=np.uint32) * 8, np.array([0x80000000], np.uint32)])
+    R = adb.tuples(np.random.default_rng(5).permutation(keys))
+    S = adb.tuples(np.random.default_rng(6).choice(keys, 70000))
+    check(oracle, algo, R, S)
 
 
 @pytest.mark.parametrize("algo", LAZY)
