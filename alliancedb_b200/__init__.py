@@ -44,6 +44,8 @@ class JoinParams(C.Structure):
         ("materialize", C.c_int32),
         ("batch_tuples", C.c_int32),
         ("seed", C.c_uint64),
+        ("realtime", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 

@@ -1,17 +1,473 @@
-// eager.cu -- eager stream joins (SHJ_*, PMJ_*).
+// eager.cu -- eager (stream) joins: SHJ_* and PMJ_* with the JM / JB / JBCR / HS
+// distribution models, over arrival-ordered relations (adb_join) and over
+// timestamped streams in tumbling windows (adb_stream_join).
+//
+// Reference:
+//   SHJ: shj() hashing/helper/localjoiner.cpp:33-59 feeds one R and one S tuple
+//        at a time; SHJJoiner::join (:73-94) inserts the tuple into its own
+//        side's table and probes the other side's table (build_hashtable_single
+//        / probe_hashtable_single, hashing/joins/common_functions.cpp:172-280).
+//   PMJ: PMJJoiner::join (localjoiner.cpp:512-600) buffers progressive_step % of
+//        each side, sorting_phase (pmj_helper.cpp:198-240) sorts the chunk pair
+//        and joins it (earlyJoinInitialRuns :11-32), and merging_phase
+//        (:188-196, earlyJoinMergedRuns :41-173) joins R of one run with S of
+//        every other run.
+//   Distribution models: the fetchers/shufflers of hashing/helper/fetcher.h:146-288
+//        and shuffler.cpp:20-168 decide which worker sees which tuple; every model
+//        yields the same matches (all twelve variants return equal counts).
+//
+// Device design.  Tuples arrive in micro-batches (batch_tuples per side).
+//   SHJ: per window two open-addressing tables HR, HS in device memory (tuple
+//        words as slots, one 64-bit CAS per insert, as in npo_join.cuh).  A batch
+//        runs two launches: R_b inserts into HR and probes HS, then S_b inserts
+//        into HS and probes HR, so every (r, s) pair is found exactly once, by
+//        whichever of the two arrived later (same batch: by s).  The models map
+//        to the table layout: JM (R replicated, S split) and HS use one shared
+//        table per side; JB (key-hash routing to nthreads joiners) splits each
+//        table into nthreads key-hash sub-tables; JBCR (groups of group_size
+//        joiners with R replicated inside a group) into nthreads / group_size
+//        sub-tables.  _P and _NP differ in the reference only in copying tuples.
+//   PMJ: each run (progressive_step % of each side) is sorted on the device
+//        (shared-memory block sort + merge-path merge passes), then joined with
+//        itself (the initial-run join) and, merge-path style, with the sorted
+//        accumulation of all earlier runs of the other side (the merged-run
+//        join, done eagerly as each run arrives), then merged into its side's
+//        accumulation.
+#include <algorithm>
+#include <chrono>
+#include <thread>
+#include <vector>
+
 #include "joins.cuh"
+#include "npo_join.cuh"
+#include "smj_sort.cuh"
 
 namespace adb {
-size_t eager_scratch(uint64_t, uint64_t, Family, uint64_t) { return 0; }
-int run_eager(Context *, const DevJoin &, Family, int, uint64_t, int, int, int, uint64_t, unsigned long long *) {
-    set_error("eager joins are not built yet");
-    return ADB_ERR_UNSUPPORTED;
-}
-int eager_set_attrs() { return ADB_OK; }
-}  // namespace adb
 
-extern "C" int adb_stream_join(const char *, const adb_stream_tuple *, uint64_t, const adb_stream_tuple *, uint64_t,
-                               const adb_join_params *, adb_window_result *, uint64_t, uint64_t *) {
-    adb::set_error("stream joins are not built yet");
-    return ADB_ERR_UNSUPPORTED;
+enum { M_JM_NP = 0, M_JM_P = 1, M_JB_NP = 2, M_JB_P = 3, M_JBCR_NP = 4, M_JBCR_P = 5, M_HS_NP = 6, M_ST = 7 };
+
+// ---------------------------------------------------------------------------
+// SHJ
+// ---------------------------------------------------------------------------
+struct ShjTables {
+    uint64_t *tab[2];          // R, S
+    uint32_t log2sub[2];       // slots per sub-table (log2)
+    uint32_t log2parts;        // sub-tables per side (log2)
+    unsigned long long *sent;  // [2] tuples equal to the empty marker, per side
+};
+
+__device__ __forceinline__ uint32_t shj_part(uint32_t key, uint32_t log2parts) {
+    return log2parts ? (uint32_t)((key * 0x85EBCA6Bu) >> (32 - log2parts)) : 0u;
 }
+
+// One micro-batch of one side: insert into the own table, probe the other.
+// `in` holds elements of `stride` 64-bit words with the tuple in the last word
+// (1: plain tuples, 2: adb_stream_tuple).
+__global__ void shj_batch(const uint64_t *__restrict__ in, uint32_t stride, uint64_t n, int side, ShjTables t,
+                          unsigned long long *acc, int *err) {
+    __shared__ uint64_t red[64];
+    const int own = side, oth = 1 - side;
+    const uint32_t lo = t.log2sub[own], lt = t.log2sub[oth];
+    const uint64_t mown = (1ULL << lo) - 1, moth = (1ULL << lt) - 1;
+    const uint64_t nsent_oth = t.sent[oth];
+    Acc a;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t w = in[i * stride + (stride - 1)];
+        const uint32_t key = tkey(w);
+        // (1)/(3): insert into the own side's table
+        if (w == kEmpty) {
+            atomicAdd(&t.sent[own], 1ull);
+        } else {
+            uint64_t *tab = t.tab[own] + ((uint64_t)shj_part(key, t.log2parts) << lo);
+            uint64_t slot = npo_hash(key, lo);
+            for (uint64_t tries = 0;; tries++) {
+                const unsigned long long prev = atomicCAS(reinterpret_cast<unsigned long long *>(tab + slot),
+                                                          (unsigned long long)kEmpty, (unsigned long long)w);
+                if (prev == kEmpty) break;
+                slot = (slot + 1) & mown;
+                if (tries > mown) { atomicExch(err, 2); break; }
+            }
+        }
+        // (2)/(4): probe the other side's table
+        const uint64_t *tab = t.tab[oth] + ((uint64_t)shj_part(key, t.log2parts) << lt);
+        uint64_t slot = npo_hash(key, lt);
+        for (uint64_t tries = 0; tries <= moth; tries++) {
+            const uint64_t v = tab[slot];
+            if (v == kEmpty) break;
+            if (tkey(v) == key) {
+                a.count++;
+                a.sum += side == 0 ? pair_hash(key, tpay(w), tpay(v)) : pair_hash(key, tpay(v), tpay(w));
+            }
+            slot = (slot + 1) & moth;
+        }
+        if (key == 0xFFFFFFFFu && nsent_oth) {
+            a.count += nsent_oth;
+            a.sum += nsent_oth * (side == 0 ? pair_hash(key, tpay(w), 0xFFFFFFFFu) : pair_hash(key, 0xFFFFFFFFu, tpay(w)));
+        }
+    }
+    block_flush(a, acc, red);
+}
+
+static uint32_t shj_log2parts(int model, int nthreads, int group_size) {
+    int parts = 1;
+    if (model == M_JB_NP || model == M_JB_P) parts = nthreads > 0 ? nthreads : 1;
+    if (model == M_JBCR_NP || model == M_JBCR_P)
+        parts = std::max(1, (nthreads > 0 ? nthreads : 1) / std::max(1, group_size > 0 ? group_size : 1));
+    uint32_t l = 0;
+    while ((1 << (l + 1)) <= parts) l++;   // round down to a power of two
+    return l;
+}
+
+static uint32_t shj_log2sub(uint64_t n, uint32_t log2parts) {
+    // two slots per tuple in each sub-table, with slack for an uneven key split
+    const uint64_t per = (n >> log2parts) + (n >> (log2parts + 1)) + 64;
+    uint32_t l = ceil_log2_u64(2 * per);
+    return l < 4 ? 4 : l;
+}
+
+// ---------------------------------------------------------------------------
+// PMJ helpers: sort a run, accumulate sorted runs
+// ---------------------------------------------------------------------------
+// Sorts n tuples of `in` (stride words per element, tuple last) into out, using
+// tmp (n words) as the ping-pong buffer.  Returns the buffer holding the result.
+__global__ void gather_tuples(const uint64_t *in, uint32_t stride, uint64_t n, uint64_t *out) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = in[i * stride + (stride - 1)];
+}
+
+static uint64_t *device_sort(Context *ctx, uint64_t *a, uint64_t *b, uint64_t n) {
+    cudaStream_t st = ctx->stream;
+    if (n == 0) return a;
+    block_sort_kernel<<<(unsigned)((n + kSortBlock - 1) / kSortBlock), 1024, kBlockSortSmem, st>>>(a, n, b);
+    ctx->kernels++;
+    uint64_t *src = b, *dst = a;
+    for (uint64_t run = kSortBlock; run < n; run *= 2) {
+        const uint64_t threads = (n + kMergeSeg - 1) / kMergeSeg;
+        merge_pass_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(src, n, run, dst);
+        ctx->kernels++;
+        std::swap(src, dst);
+    }
+    return src;
+}
+
+static void launch_merge_join(Context *ctx, const uint64_t *A, uint64_t na, const uint64_t *B, uint64_t nb,
+                              int a_is_r, unsigned long long *acc) {
+    if (!na || !nb) return;
+    const uint64_t threads = (na + nb + kMergeSeg - 1) / kMergeSeg;
+    merge_join_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, ctx->stream>>>(A, na, B, nb, a_is_r, acc);
+    ctx->kernels++;
+}
+
+static void launch_merge(Context *ctx, const uint64_t *A, uint64_t na, const uint64_t *B, uint64_t nb, uint64_t *out) {
+    const uint64_t threads = (na + nb + kMergeSeg - 1) / kMergeSeg;
+    if (!threads) return;
+    merge_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, ctx->stream>>>(A, na, B, nb, out);
+    ctx->kernels++;
+}
+
+// State of one window of an eager join.
+struct EagerWindow {
+    // SHJ
+    ShjTables t;
+    uint64_t tab_slots[2];
+    // PMJ: sorted accumulations (double-buffered) and run scratch
+    uint64_t *accum[2][2];
+    uint64_t n_accum[2];
+    int cur[2];
+    uint64_t *run_a, *run_b;
+};
+
+struct EagerPlan {
+    Family fam;
+    uint32_t log2parts;
+    uint32_t log2sub[2];
+    uint64_t capR, capS;   // most tuples of one window
+    uint64_t run_cap;      // PMJ: most tuples of one run
+};
+
+static EagerPlan plan_eager(Family fam, int model, int nthreads, int group_size, uint64_t capR, uint64_t capS,
+                            uint64_t run_cap) {
+    EagerPlan p{};
+    p.fam = fam;
+    p.capR = capR;
+    p.capS = capS;
+    p.run_cap = run_cap;
+    if (fam == Family::Shj) {
+        p.log2parts = shj_log2parts(model, nthreads, group_size);
+        p.log2sub[0] = shj_log2sub(capR, p.log2parts);
+        p.log2sub[1] = shj_log2sub(capS, p.log2parts);
+    }
+    return p;
+}
+
+static size_t eager_plan_bytes(const EagerPlan &p) {
+    if (p.fam == Family::Shj)
+        return Workspace::need(1ULL << (p.log2sub[0] + p.log2parts), 8) +
+               Workspace::need(1ULL << (p.log2sub[1] + p.log2parts), 8) + Workspace::need(2, 8);
+    return 2 * Workspace::need(p.capR + 1, 8) + 2 * Workspace::need(p.capS + 1, 8) +
+           2 * Workspace::need(p.run_cap + 1, 8);
+}
+
+static void take_window(Context *ctx, const EagerPlan &p, EagerWindow &w) {
+    if (p.fam == Family::Shj) {
+        for (int s = 0; s < 2; s++) {
+            w.tab_slots[s] = 1ULL << (p.log2sub[s] + p.log2parts);
+            w.t.tab[s] = ctx->ws.take<uint64_t>(w.tab_slots[s]);
+            w.t.log2sub[s] = p.log2sub[s];
+        }
+        w.t.log2parts = p.log2parts;
+        w.t.sent = ctx->ws.take<unsigned long long>(2);
+    } else {
+        for (int s = 0; s < 2; s++) {
+            const uint64_t cap = s ? p.capS : p.capR;
+            w.accum[s][0] = ctx->ws.take<uint64_t>(cap + 1);
+            w.accum[s][1] = ctx->ws.take<uint64_t>(cap + 1);
+        }
+        w.run_a = ctx->ws.take<uint64_t>(p.run_cap + 1);
+        w.run_b = ctx->ws.take<uint64_t>(p.run_cap + 1);
+    }
+}
+
+static int reset_window(Context *ctx, const EagerPlan &p, EagerWindow &w) {
+    if (p.fam == Family::Shj) {
+        for (int s = 0; s < 2; s++) ADB_CK(cudaMemsetAsync(w.t.tab[s], 0xFF, w.tab_slots[s] * 8, ctx->stream));
+        ADB_CK(cudaMemsetAsync(w.t.sent, 0, 16, ctx->stream));
+    } else {
+        w.n_accum[0] = w.n_accum[1] = 0;
+        w.cur[0] = w.cur[1] = 0;
+    }
+    return ADB_OK;
+}
+
+static int grid_for(Context *ctx, uint64_t n) {
+    uint64_t b = (n + 255) / 256;
+    const uint64_t cap = (uint64_t)ctx->num_sms * 8;
+    return (int)(b < 1 ? 1 : (b > cap ? cap : b));
+}
+
+// SHJ: one micro-batch of each side, R first (shj() alternates R then S).
+static int shj_step(Context *ctx, EagerWindow &w, const uint64_t *R, uint64_t nr, const uint64_t *S, uint64_t ns,
+                    uint32_t stride, unsigned long long *acc) {
+    cudaStream_t st = ctx->stream;
+    int *err = reinterpret_cast<int *>(acc + 2);
+    if (nr) {
+        shj_batch<<<grid_for(ctx, nr), 256, 0, st>>>(R, stride, nr, 0, w.t, acc, err);
+        ctx->kernels++;
+    }
+    if (ns) {
+        shj_batch<<<grid_for(ctx, ns), 256, 0, st>>>(S, stride, ns, 1, w.t, acc, err);
+        ctx->kernels++;
+    }
+    ADB_CK(cudaGetLastError());
+    return ADB_OK;
+}
+
+// PMJ: one run of each side.
+static int pmj_step(Context *ctx, EagerWindow &w, const uint64_t *R, uint64_t nr, const uint64_t *S, uint64_t ns,
+                    uint32_t stride, unsigned long long *acc) {
+    cudaStream_t st = ctx->stream;
+    // sorted run of R -> run_a/run_b; keep the sorted copy in place, sort S into
+    // the accumulation's spare buffer region afterwards
+    const uint64_t *run_sorted[2] = {nullptr, nullptr};
+    uint64_t nrun[2] = {nr, ns};
+    // sort R's run
+    uint64_t *rs = nullptr, *ss = nullptr;
+    if (nr) {
+        gather_tuples<<<grid_for(ctx, nr), 256, 0, st>>>(R, stride, nr, w.run_a);
+        ctx->kernels++;
+        rs = device_sort(ctx, w.run_a, w.run_b, nr);
+    }
+    // S's run goes through the spare accumulation buffer of S as scratch
+    uint64_t *s_spare = w.accum[1][w.cur[1] ^ 1];
+    uint64_t *r_spare = w.accum[0][w.cur[0] ^ 1];
+    if (ns) {
+        // two scratch halves: the other run buffer and the spare accumulation of R
+        uint64_t *a = rs == w.run_a ? w.run_b : w.run_a;
+        gather_tuples<<<grid_for(ctx, ns), 256, 0, st>>>(S, stride, ns, a);
+        ctx->kernels++;
+        ss = device_sort(ctx, a, s_spare, ns);
+        if (ss == s_spare) {   // keep the sorted S run out of the spare buffer, which the merge below writes
+            ADB_CK(cudaMemcpyAsync(a, s_spare, ns * 8, cudaMemcpyDeviceToDevice, st));
+            ss = a;
+        }
+    }
+    run_sorted[0] = rs;
+    run_sorted[1] = ss;
+    // initial-run join (earlyJoinInitialRuns) and merged-run joins against the
+    // earlier runs of the other side (earlyJoinMergedRuns), eagerly
+    launch_merge_join(ctx, rs, nr, ss, ns, 1, acc);
+    launch_merge_join(ctx, w.accum[0][w.cur[0]], w.n_accum[0], ss, ns, 1, acc);
+    launch_merge_join(ctx, w.accum[1][w.cur[1]], w.n_accum[1], rs, nr, 0, acc);
+    // accumulate: merge each sorted run into its side's sorted accumulation
+    for (int s = 0; s < 2; s++) {
+        if (!nrun[s]) continue;
+        uint64_t *spare = s ? s_spare : r_spare;
+        launch_merge(ctx, w.accum[s][w.cur[s]], w.n_accum[s], run_sorted[s], nrun[s], spare);
+        w.cur[s] ^= 1;
+        w.n_accum[s] += nrun[s];
+    }
+    ADB_CK(cudaGetLastError());
+    return ADB_OK;
+}
+
+static int eager_step(Context *ctx, const EagerPlan &p, EagerWindow &w, const uint64_t *R, uint64_t nr,
+                      const uint64_t *S, uint64_t ns, uint32_t stride, unsigned long long *acc) {
+    return p.fam == Family::Shj ? shj_step(ctx, w, R, nr, S, ns, stride, acc)
+                                : pmj_step(ctx, w, R, nr, S, ns, stride, acc);
+}
+
+// ---------------------------------------------------------------------------
+// Relations given as arrival sequences (adb_join with an eager algorithm name)
+// ---------------------------------------------------------------------------
+static void eager_steps(Family fam, uint64_t nR, uint64_t nS, uint64_t batch, int progressive_step, uint64_t *sr,
+                        uint64_t *ss) {
+    if (fam == Family::Shj) {
+        // micro-batches of `batch` tuples per side, at most 256 of them
+        uint64_t b = std::max<uint64_t>(batch, 1);
+        b = std::max<uint64_t>(b, (std::max(nR, nS) + 255) / 256);
+        *sr = *ss = b;
+    } else {
+        // launcher.cpp:38-43: progressive_step % of each side per run
+        const uint64_t ps = progressive_step > 0 ? (uint64_t)progressive_step : 1;
+        *sr = std::max<uint64_t>(1, nR * ps / 100);
+        *ss = std::max<uint64_t>(1, nS * ps / 100);
+    }
+}
+
+size_t eager_scratch(uint64_t nR, uint64_t nS, Family fam, int model, int nthreads, int group_size) {
+    return eager_plan_bytes(plan_eager(fam, model, nthreads, group_size, nR, nS, std::max(nR, nS)));
+}
+
+int run_eager(Context *ctx, const DevJoin &j, Family fam, int model, uint64_t batch, int nthreads, int group_size,
+              int progressive_step, uint64_t /*seed*/, unsigned long long *acc) {
+    uint64_t sr, ss;
+    eager_steps(fam, j.nR, j.nS, batch, progressive_step, &sr, &ss);
+    const uint64_t runs = std::max((j.nR + sr - 1) / sr, (j.nS + ss - 1) / ss);
+    const EagerPlan p = plan_eager(fam, model, nthreads, group_size, j.nR, j.nS, std::max(j.nR, j.nS));
+    EagerWindow w;
+    take_window(ctx, p, w);
+    ADB_TRY(reset_window(ctx, p, w));
+    ADB_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    ADB_CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+    ADB_CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+    for (uint64_t k = 0; k < runs; k++) {
+        // the last step takes the left-over of both sides (localjoiner.cpp:575-590)
+        const uint64_t r0 = std::min(j.nR, k * sr), r1 = k + 1 == runs ? j.nR : std::min(j.nR, (k + 1) * sr);
+        const uint64_t s0 = std::min(j.nS, k * ss), s1 = k + 1 == runs ? j.nS : std::min(j.nS, (k + 1) * ss);
+        ADB_TRY(eager_step(ctx, p, w, j.R + r0, r1 - r0, j.S + s0, s1 - s0, 1, acc));
+    }
+    return ADB_OK;
+}
+
+int eager_set_attrs() {
+    ADB_CK(cudaFuncSetAttribute(block_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kBlockSortSmem));
+    return ADB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Timestamped streams in tumbling windows
+// ---------------------------------------------------------------------------
+int stream_join(Context *ctx, Family fam, int model, const adb_stream_tuple *R, uint64_t nR,
+                const adb_stream_tuple *S, uint64_t nS, const adb_join_params *p, adb_window_result *out,
+                uint64_t max_windows, uint64_t *n_windows) {
+    cudaStream_t st = ctx->stream;
+    const uint64_t W = p && p->window_size > 0 ? (uint64_t)p->window_size : 1000;
+    const uint64_t batch = p && p->batch_tuples > 0 ? (uint64_t)p->batch_tuples : 1600;
+    const int nthreads = p && p->nthreads ? (int)p->nthreads : 1;
+    const int group_size = p ? p->group_size : 0;
+    const int pstep = p && p->progressive_step > 0 ? p->progressive_step : 1;
+    const bool realtime = p && p->realtime;
+    *n_windows = 0;
+    if (!nR && !nS) return ADB_OK;
+    // window boundaries from the timestamps (both streams are ts-ordered)
+    const uint64_t t0 = std::min(nR ? R[0].ts_ms : ~0ULL, nS ? S[0].ts_ms : ~0ULL);
+    const uint64_t tend = std::max(nR ? R[nR - 1].ts_ms : 0ULL, nS ? S[nS - 1].ts_ms : 0ULL);
+    const uint64_t wbase = t0 / W * W;
+    const uint64_t nwin = (tend - wbase) / W + 1;
+    std::vector<uint64_t> rb(nwin + 1), sb(nwin + 1);
+    {
+        uint64_t i = 0, k = 0;
+        for (uint64_t w = 0; w <= nwin; w++) {
+            const uint64_t lim = wbase + w * W;
+            while (i < nR && R[i].ts_ms < lim) i++;
+            while (k < nS && S[k].ts_ms < lim) k++;
+            rb[w] = i;
+            sb[w] = k;
+        }
+        rb[nwin] = nR;
+        sb[nwin] = nS;
+    }
+    uint64_t capR = 0, capS = 0;
+    for (uint64_t w = 0; w < nwin; w++) {
+        capR = std::max(capR, rb[w + 1] - rb[w]);
+        capS = std::max(capS, sb[w + 1] - sb[w]);
+    }
+    const EagerPlan plan = plan_eager(fam, model, nthreads, group_size, capR, capS, std::max(capR, capS));
+    const size_t in_bytes = Workspace::need(nR + 1, 16) + Workspace::need(nS + 1, 16);
+    ADB_TRY(ctx->ws.reserve(in_bytes + eager_plan_bytes(plan) + 4096));
+    uint64_t *dR = reinterpret_cast<uint64_t *>(ctx->ws.take<adb_stream_tuple>(nR + 1));
+    uint64_t *dS = reinterpret_cast<uint64_t *>(ctx->ws.take<adb_stream_tuple>(nS + 1));
+    unsigned long long *acc = ctx->ws.take<unsigned long long>(4);
+    EagerWindow win;
+    take_window(ctx, plan, win);
+    if (nR) ADB_CK(cudaMemcpyAsync(dR, R, nR * 16, cudaMemcpyHostToDevice, st));
+    if (nS) ADB_CK(cudaMemcpyAsync(dS, S, nS * 16, cudaMemcpyHostToDevice, st));
+    ADB_CK(cudaStreamSynchronize(st));
+
+    const auto wall0 = std::chrono::steady_clock::now();
+    for (uint64_t w = 0; w < nwin; w++) {
+        const uint64_t r0 = rb[w], r1 = rb[w + 1], s0 = sb[w], s1 = sb[w + 1];
+        ADB_TRY(reset_window(ctx, plan, win));
+        ADB_CK(cudaMemsetAsync(acc, 0, 32, st));
+        // micro-batches: SHJ `batch` tuples per side, PMJ progressive_step % runs
+        uint64_t sr = batch, ss = batch;
+        if (fam == Family::Pmj) {
+            sr = std::max<uint64_t>(1, (r1 - r0) * pstep / 100);
+            ss = std::max<uint64_t>(1, (s1 - s0) * pstep / 100);
+        }
+        const uint64_t steps = std::max<uint64_t>(1, std::max((r1 - r0 + sr - 1) / sr, (s1 - s0 + ss - 1) / ss));
+        for (uint64_t k = 0; k < steps; k++) {
+            const uint64_t a0 = std::min(r1, r0 + k * sr), a1 = k + 1 == steps ? r1 : std::min(r1, r0 + (k + 1) * sr);
+            const uint64_t c0 = std::min(s1, s0 + k * ss), c1 = k + 1 == steps ? s1 : std::min(s1, s0 + (k + 1) * ss);
+            if (realtime) {
+                // release the batch when its last tuple has arrived (WAIT, fetcher.cpp:120-190)
+                uint64_t last = 0;
+                if (a1 > a0) last = std::max(last, R[a1 - 1].ts_ms);
+                if (c1 > c0) last = std::max(last, S[c1 - 1].ts_ms);
+                const auto due = wall0 + std::chrono::milliseconds(last - t0);
+                std::this_thread::sleep_until(due);
+            }
+            if (k + 1 == steps) ADB_CK(cudaEventRecord(ctx->ev[4], st));
+            ADB_TRY(eager_step(ctx, plan, win, dR + 2 * a0, a1 - a0, dS + 2 * c0, c1 - c0, 2, acc));
+        }
+        const auto close = std::chrono::steady_clock::now();
+        ADB_CK(cudaMemcpyAsync(ctx->h_res, acc, 32, cudaMemcpyDeviceToHost, st));
+        ADB_CK(cudaEventRecord(ctx->ev[5], st));
+        ADB_CK(cudaStreamSynchronize(st));
+        if (ctx->h_res[2]) {
+            set_error("device table overflow in window %llu", (unsigned long long)w);
+            return ADB_ERR_DEVICE;
+        }
+        if (w < max_windows && out) {
+            adb_window_result &o = out[w];
+            o.window_start_ms = wbase + w * W;
+            o.n_r = r1 - r0;
+            o.n_s = s1 - s0;
+            o.count = ctx->h_res[0];
+            o.checksum = ctx->h_res[1];
+            float ms = 0;
+            if (realtime) {
+                ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - close).count();
+            } else {
+                cudaEventElapsedTime(&ms, ctx->ev[4], ctx->ev[5]);
+            }
+            o.latency_ms = ms;
+            o.reserved = 0;
+        }
+    }
+    *n_windows = nwin;
+    return ADB_OK;
+}
+
+}  // namespace adb

@@ -196,7 +196,9 @@ static size_t scratch_for(const AlgoEntry *a, uint64_t nR, uint64_t nS, const ad
         case Family::Npo: return npo_scratch(nR);
         case Family::SortMerge: return smj_scratch(nR, nS, p ? p->part_fanout : 0, num_sms);
         case Family::Shj:
-        case Family::Pmj: return eager_scratch(nR, nS, a->fam, eager_batch(p));
+        case Family::Pmj:
+            return eager_scratch(nR, nS, a->fam, a->model, p && p->nthreads ? (int)p->nthreads : 1,
+                                 p ? p->group_size : 0);
         default: return 0;
     }
 }
@@ -375,6 +377,29 @@ int adb_join(const char *algo, const adb_tuple *R, uint64_t nR, const adb_tuple 
     float th = 0;
     if (cudaEventElapsedTime(&th, ctx->ev[4], ctx->ev[5]) == cudaSuccess) out->ms_h2d = th;
     return out->status = s;
+}
+
+int adb_stream_join(const char *algo, const adb_stream_tuple *R, uint64_t nR, const adb_stream_tuple *S,
+                    uint64_t nS, const adb_join_params *p, adb_window_result *windows, uint64_t max_windows,
+                    uint64_t *n_windows) {
+    if (!n_windows) { set_error("n_windows is NULL"); return ADB_ERR_ARG; }
+    *n_windows = 0;
+    const AlgoEntry *a = find_algo(algo);
+    if (!a) { set_error("unknown algorithm '%s'", algo ? algo : "(null)"); return ADB_ERR_ARG; }
+    if (a->fam != Family::Shj && a->fam != Family::Pmj) {
+        set_error("%s is not an eager stream join (SHJ_* or PMJ_*)", a->name);
+        return ADB_ERR_ARG;
+    }
+    if ((nR && !R) || (nS && !S) || (max_windows && !windows)) { set_error("NULL pointer"); return ADB_ERR_ARG; }
+    for (uint64_t i = 1; i < nR; i++)
+        if (R[i].ts_ms < R[i - 1].ts_ms) { set_error("R is not ordered by timestamp (index %llu)", (unsigned long long)i); return ADB_ERR_ARG; }
+    for (uint64_t i = 1; i < nS; i++)
+        if (S[i].ts_ms < S[i - 1].ts_ms) { set_error("S is not ordered by timestamp (index %llu)", (unsigned long long)i); return ADB_ERR_ARG; }
+    int s;
+    Context *ctx = ctx_get(&s);
+    if (!ctx) return s;
+    ctx->kernels = 0;
+    return stream_join(ctx, a->fam, a->model, R, nR, S, nS, p, windows, max_windows, n_windows);
 }
 
 int adb_device_alloc(void **ptr, size_t bytes) {

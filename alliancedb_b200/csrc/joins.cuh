@@ -46,8 +46,11 @@ size_t smj_scratch(uint64_t nR, uint64_t nS, int part_fanout, int num_sms);
 int run_smj(Context *ctx, const DevJoin &j, int part_fanout, bool multipass, unsigned long long *acc);
 
 // ---- eager SHJ / PMJ over one window given as arrival-ordered relations ----
-size_t eager_scratch(uint64_t nR, uint64_t nS, Family fam, uint64_t batch);
+size_t eager_scratch(uint64_t nR, uint64_t nS, Family fam, int model, int nthreads, int group_size);
 int run_eager(Context *ctx, const DevJoin &j, Family fam, int model, uint64_t batch, int nthreads,
               int group_size, int progressive_step, uint64_t seed, unsigned long long *acc);
+int stream_join(Context *ctx, Family fam, int model, const adb_stream_tuple *R, uint64_t nR,
+                const adb_stream_tuple *S, uint64_t nS, const adb_join_params *p, adb_window_result *out,
+                uint64_t max_windows, uint64_t *n_windows);
 
 }  // namespace adb

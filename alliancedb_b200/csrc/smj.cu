@@ -24,6 +24,7 @@
 #include "joins.cuh"
 #include "paged.cuh"
 #include "radix_join.cuh"
+#include "smj_sort.cuh"
 
 namespace adb {
 
@@ -31,7 +32,6 @@ constexpr uint32_t kSmjCap = 8192;                  // tuples per R chunk and pe
 constexpr uint32_t kSmjChunkW = kSmjCap - kPageTuples;
 constexpr uint32_t kSmjSPages = kSmjCap / kPageTuples;   // 128 pages <= 8192 tuples
 constexpr uint32_t kSmjMaxPages = 272;              // weight floor 32: <= 8192 / 32 + 1 pages per chunk
-constexpr uint32_t kSmjBucketBits = 12;
 constexpr uint32_t kSmjThreads = 1024;
 
 // A | B | C tuple buffers, bucket counters, R page table, barrier and scratch.
@@ -55,106 +55,6 @@ struct SmjArgs {
     unsigned long long *mat_n;
     uint64_t mat_cap;
 };
-
-// Sorts src[0..n) by key into dst (both shared memory).  cnt holds 2^12 + 1
-// counters; red holds 64 scratch words.  All threads call it.
-__device__ void chunk_sort(const uint64_t *src, uint32_t n, uint64_t *dst, uint32_t *cnt, uint32_t *red) {
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    // key bits that differ within the chunk
-    uint32_t a = 0xFFFFFFFFu, o = 0;
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-        const uint32_t k = tkey(src[i]);
-        a &= k;
-        o |= k;
-    }
-#pragma unroll
-    for (int s = 16; s > 0; s >>= 1) {
-        a &= __shfl_xor_sync(0xffffffffu, a, s);
-        o |= __shfl_xor_sync(0xffffffffu, o, s);
-    }
-    if (lane == 0) { red[wid] = a; red[32 + wid] = o; }
-    __syncthreads();
-    a = 0xFFFFFFFFu;
-    o = 0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); w++) { a &= red[w]; o |= red[32 + w]; }
-    const uint32_t vary = a ^ o;
-    __syncthreads();
-    if (vary == 0) {   // one key value: already sorted
-        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
-        __syncthreads();
-        return;
-    }
-    const uint32_t hi = 31 - __clz(vary);
-    const uint32_t nbits = hi + 1 < kSmjBucketBits ? hi + 1 : kSmjBucketBits;
-    const uint32_t shift = hi + 1 - nbits;
-    const uint32_t nb = 1u << nbits, bmask = nb - 1;
-    for (uint32_t d = threadIdx.x; d < nb; d += blockDim.x) cnt[d] = 0;
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) atomicAdd(&cnt[(tkey(src[i]) >> shift) & bmask], 1u);
-    __syncthreads();
-    {   // exclusive scan of the bucket counts, contiguous buckets per thread
-        const uint32_t per = (nb + blockDim.x - 1) / blockDim.x;
-        const uint32_t d0 = threadIdx.x * per, d1 = min(nb, d0 + per);
-        uint32_t loc = 0;
-        for (uint32_t d = d0; d < d1; d++) loc += cnt[d];
-        uint32_t tot;
-        uint32_t ex = block_exclusive_scan(loc, red, &tot);
-        for (uint32_t d = d0; d < d1; d++) {
-            const uint32_t c = cnt[d];
-            cnt[d] = ex;
-            ex += c;
-        }
-    }
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-        const uint64_t v = src[i];
-        dst[atomicAdd(&cnt[(tkey(v) >> shift) & bmask], 1u)] = v;
-    }
-    __syncthreads();
-    // cnt[d] is now the end of bucket d.  Buckets of more than 128 tuples
-    // (keys clustered below the bucket bits) would make the insertion sort
-    // quadratic: then the whole chunk is bitonic-sorted on the 64-bit word
-    // instead, padded with all-ones words that sort last.
-    if (shift) {
-        int big = 0;
-        for (uint32_t d = threadIdx.x; d < nb; d += blockDim.x)
-            if (cnt[d] - (d ? cnt[d - 1] : 0u) > 128) big = 1;
-        if (__syncthreads_or(big)) {
-            uint32_t m = 1;
-            while (m < n) m <<= 1;
-            for (uint32_t i = n + threadIdx.x; i < m; i += blockDim.x) dst[i] = ~0ULL;
-            __syncthreads();
-            for (uint32_t k = 2; k <= m; k <<= 1) {
-                for (uint32_t jj = k >> 1; jj > 0; jj >>= 1) {
-                    for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
-                        const uint32_t l = i ^ jj;
-                        if (l > i) {
-                            const uint64_t x = dst[i], y = dst[l];
-                            const bool up = (i & k) == 0;
-                            if ((x > y) == up) { dst[i] = y; dst[l] = x; }
-                        }
-                    }
-                    __syncthreads();
-                }
-            }
-            return;
-        }
-        for (uint32_t d = threadIdx.x; d < nb; d += blockDim.x) {
-            const uint32_t b = d ? cnt[d - 1] : 0u, e = cnt[d];
-            for (uint32_t i = b + 1; i < e; i++) {
-                const uint64_t v = dst[i];
-                const uint32_t k = tkey(v);
-                uint32_t j = i;
-                while (j > b && tkey(dst[j - 1]) > k) {
-                    dst[j] = dst[j - 1];
-                    j--;
-                }
-                dst[j] = v;
-            }
-        }
-        __syncthreads();
-    }
-}
 
 __global__ void __launch_bounds__(kSmjThreads, 1)
 smj_items(SmjArgs a) {

@@ -80,6 +80,9 @@ typedef struct adb_join_params {
     int32_t materialize;        /* 1: also write <S-key, S-payload> per match (JOIN_RESULT_MATERIALIZE) */
     int32_t batch_tuples;       /* eager joins: arrival micro-batch in tuples per side; 0 = 1 ms of stream */
     uint64_t seed;              /* JBCR's random split of S */
+    int32_t realtime;           /* adb_stream_join: 1 = release each micro-batch at its timestamp
+                                   (wall clock, the reference's WAIT gating, fetcher.cpp:120-190) */
+    int32_t reserved;
 } adb_join_params;
 
 typedef struct adb_join_result {
