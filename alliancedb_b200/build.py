@@ -65,13 +65,15 @@ def build_cuda(verbose: bool = False) -> Path:
     return LIB
 
 
+REF_SRC = Path("/root/reference/hashing")
+
+
 def build_oracle() -> Path:
-    src = ROOT / "oracle" / "adb_oracle.c"
-    hdr = ROOT / "oracle" / "adb_oracle.h"
-    if _newer(src, ORACLE_LIB, [hdr]):
-        tmp = ORACLE_LIB.with_suffix(".so.tmp")
-        _run(["gcc", "-O2", "-std=c11", "-shared", "-fPIC", "-o", str(tmp), str(src)])
-        os.replace(tmp, ORACLE_LIB)
+    """The CPU checker: the C restatement, and (when the AllianceDB sources are
+    present on this machine) the reference's own joins under oracle/_ref/."""
+    _run(["make", "-s", "-C", str(ROOT / "oracle"), "liboracle.so"])
+    if REF_SRC.is_dir():
+        _run(["make", "-s", "-C", str(ROOT / "oracle"), "ref", f"REF_SRC={REF_SRC}"])
     return ORACLE_LIB
 
 

@@ -1,0 +1,177 @@
+// harness.cpp -- TEST INFRASTRUCTURE ONLY.  Drives the reference's own join
+// functions (compiled unmodified from hashing/ by oracle/Makefile) for two
+// purposes: the reference counts the tests pin against, and the CPU baseline
+// (bench.py --impl reference) timed on the host's cores.
+//
+// Usage:
+//   adb_ref_bench <PRO|PRH|RJ_st|NPO|NPO_st> gen <n> <threads> <reps>
+//       PK-FK relations of n tuples each (R keys a seeded permutation of 1..n,
+//       S keys drawn uniformly from R's keys; the generator of the benchmark
+//       configs, restated here), one warm-up call, then reps timed calls
+//   adb_ref_bench <algo> files <R.bin> <S.bin> <threads>
+//       relations from files of 8-byte {payload, key} tuples, one call
+// Prints one JSON line: algo, n_r, n_s, threads, count, ms (median), tuples_per_s.
+//
+// Platform utilities the reference links against (CPU pinning, NUMA queries,
+// the global thread count of hashing/utils/generator.cpp:57) are provided
+// below: identity CPU mapping over the online cores, one NUMA node.
+#include <unistd.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <fstream>
+#include <string>
+#include <vector>
+
+#include "joins/no_partitioning_join.h"
+#include "joins/parallel_radix_join.h"
+#include "joins/prj_params.h"
+#include "utils/generator.h"
+
+int nthreads = 1;
+int numalocalize = 0;
+
+int get_cpu_id(int thread_id) { return thread_id % (int)sysconf(_SC_NPROCESSORS_ONLN); }
+int get_numa_id(int) { return 0; }
+int get_num_numa_regions(void) { return 1; }
+int get_numa_node_of_address(void *) { return 0; }
+int numa_localize(tuple_t *, int64_t, uint32_t) { return 0; }
+void *alloc_aligned(size_t size) {
+    void *p = nullptr;
+    if (posix_memalign(&p, 64, size)) return nullptr;
+    return p;
+}
+
+// ---- the benchmark generator (counter-based; see alliancedb_b200/csrc/datagen.cuh)
+static uint64_t fmix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+static uint64_t mix3(uint64_t seed, uint64_t stream, uint64_t i) {
+    return fmix64(fmix64(seed + stream * 0x632BE59BD9B4E019ULL) ^ (i * 0x9E3779B97F4A7C15ULL + 1));
+}
+struct Feistel {
+    uint64_t n, hmask;
+    uint32_t half;
+    uint64_t k[4];
+    Feistel(uint64_t n_, uint64_t seed) : n(n_) {
+        uint32_t bits = 2;
+        while (bits < 64 && (1ULL << bits) < n_) bits++;
+        bits = (bits + 1) & ~1u;
+        half = bits / 2;
+        hmask = (1ULL << half) - 1;
+        for (int r = 0; r < 4; r++) k[r] = mix3(seed, 1000 + r, 0);
+    }
+    uint64_t once(uint64_t x) const {
+        uint64_t L = x >> half, R = x & hmask;
+        for (int r = 0; r < 4; r++) {
+            const uint64_t t = R;
+            R = L ^ (fmix64(k[r] ^ R) & hmask);
+            L = t;
+        }
+        return (L << half) | R;
+    }
+    uint64_t operator()(uint64_t i) const {
+        uint64_t x = once(i);
+        while (x >= n) x = once(x);
+        return x;
+    }
+};
+
+static tuple_t *alloc_rel(uint64_t n) {
+    // the reference allocates RELATION_PADDING of slack behind every relation,
+    // which PRO uses as partitioning space (hashing/benchmark.cpp:15-17, 60)
+    return (tuple_t *)alloc_aligned(n * sizeof(tuple_t) + RELATION_PADDING);
+}
+
+static void gen_pkfk(uint64_t n, std::vector<tuple_t> &R, std::vector<tuple_t> &S) {
+    R.resize(n);
+    S.resize(n);
+    Feistel perm(n ? n : 1, 1);
+    for (uint64_t i = 0; i < n; i++) {
+        R[i].payloadID = (int32_t)i;
+        R[i].key = (int32_t)(1 + perm(i));
+    }
+    for (uint64_t j = 0; j < n; j++) {
+        const uint64_t idx = (uint64_t)(((unsigned __int128)mix3(2, 3, j) * n) >> 64);
+        S[j].payloadID = (int32_t)j;
+        S[j].key = R[idx].key;
+    }
+}
+
+static bool read_rel(const char *path, std::vector<tuple_t> &out) {
+    std::ifstream f(path, std::ios::binary | std::ios::ate);
+    if (!f) return false;
+    const std::streamsize bytes = f.tellg();
+    f.seekg(0);
+    out.resize(bytes / sizeof(tuple_t));
+    f.read(reinterpret_cast<char *>(out.data()), (std::streamsize)(out.size() * sizeof(tuple_t)));
+    return (bool)f;
+}
+
+typedef result_t *(*join_fn)(relation_t *, relation_t *, param_t);
+
+int main(int argc, char **argv) {
+    if (argc < 3) {
+        fprintf(stderr, "usage: %s <algo> gen <n> <threads> <reps> | <algo> files <R> <S> <threads>\n", argv[0]);
+        return 2;
+    }
+    const std::string algo = argv[1];
+    join_fn fn = algo == "PRO"      ? PRO
+                 : algo == "PRH"    ? PRH
+                 : algo == "RJ_st"  ? RJ_st
+                 : algo == "NPO"    ? NPO
+                 : algo == "NPO_st" ? NPO_st
+                                    : nullptr;
+    if (!fn) {
+        fprintf(stderr, "unsupported algorithm %s\n", algo.c_str());
+        return 2;
+    }
+    std::vector<tuple_t> R0, S0;
+    int reps = 1;
+    if (std::string(argv[2]) == "gen" && argc >= 6) {
+        gen_pkfk(strtoull(argv[3], nullptr, 10), R0, S0);
+        nthreads = atoi(argv[4]);
+        reps = atoi(argv[5]);
+    } else if (std::string(argv[2]) == "files" && argc >= 6) {
+        if (!read_rel(argv[3], R0) || !read_rel(argv[4], S0)) {
+            fprintf(stderr, "cannot read relations\n");
+            return 2;
+        }
+        nthreads = atoi(argv[5]);
+    } else {
+        return 2;
+    }
+    if (nthreads < 1) nthreads = 1;
+    param_t p;
+    memset((void *)&p, 0, sizeof(p));
+    p.nthreads = nthreads;
+    p.duplicate_num = 1;
+    p.progressive_step = 1;
+    p.merge_step = 2;
+    tuple_t *rt = alloc_rel(R0.size()), *st = alloc_rel(S0.size());
+    std::vector<double> ms;
+    int64_t count = -1;
+    for (int r = 0; r < reps + (reps > 1 ? 1 : 0); r++) {
+        // fresh copies: PRO overwrites its inputs (parallel_radix_join.cpp:1176-1181)
+        memcpy(rt, R0.data(), R0.size() * sizeof(tuple_t));
+        memcpy(st, S0.data(), S0.size() * sizeof(tuple_t));
+        relation_t relR{rt, R0.size(), nullptr}, relS{st, S0.size(), nullptr};
+        const auto t0 = std::chrono::steady_clock::now();
+        result_t *res = fn(&relR, &relS, p);
+        const auto t1 = std::chrono::steady_clock::now();
+        count = res ? res->totalresults : -1;
+        free(res);
+        if (reps > 1 && r == 0) continue;   // warm-up
+        ms.push_back(std::chrono::duration<double, std::milli>(t1 - t0).count());
+    }
+    std::sort(ms.begin(), ms.end());
+    const double med = ms[ms.size() / 2];
+    printf("{\"algo\": \"%s\", \"n_r\": %zu, \"n_s\": %zu, \"threads\": %d, \"count\": %lld, \"ms\": %.3f, "
+           "\"tuples_per_s\": %.1f}\n",
+           algo.c_str(), R0.size(), S0.size(), nthreads, (long long)count, med,
+           (R0.size() + S0.size()) / (med / 1e3));
+    return 0;
+}

@@ -134,3 +134,17 @@ def test_inputs_not_modified():
     R0, S0 = R.copy(), S.copy()
     adb.join("PRO", R, S)
     assert np.array_equal(R, R0) and np.array_equal(S, S0)
+
+
+@pytest.mark.parametrize("algo", LAZY + ["SHJ_JM_NP", "SHJ_JB_NP", "PMJ_JM_NP", "PMJ_JBCR_NP"])
+def test_golden_fixtures(algo):
+    """Results equal the committed fixtures, whose counts the reference itself produced."""
+    import json
+    from pathlib import Path
+    golden = Path(__file__).resolve().parent / "golden"
+    meta = json.loads((golden / "cases.json").read_text())
+    for name, m in meta.items():
+        R = np.load(golden / f"{name}_R.npy")
+        S = np.load(golden / f"{name}_S.npy")
+        got = adb.join(algo, R, S, adb.default_params(batch_tuples=64, nthreads=4, progressive_step=10))
+        assert (got.count, got.checksum) == (m["count"], int(m["checksum"])), name

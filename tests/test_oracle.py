@@ -1,0 +1,119 @@
+"""The CPU oracle, pinned before it is trusted (no GPU needed).
+
+* every restatement (PRO, PRH, NPO, SMJ, SHJ, PMJ) equals the independent
+  sort-based truth on seeded and edge-case inputs;
+* the golden fixtures: the reference's own PRO / PRH / RJ_st / NPO / NPO_st
+  counts (recorded from oracle/_ref, the reference compiled unmodified) equal
+  the truth's count, and the oracle reproduces the recorded checksums;
+* known answers: a PK-FK join matches every S tuple once (hashing/test/test.cpp:72)
+  and its checksum has a closed form from the generator's drawn indices;
+* when the reference binary is present, it is re-run on fresh inputs.
+"""
+import json
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import alliancedb_b200 as adb
+from tests.golden.make_golden import cases as golden_cases
+from tests.golden.make_golden import fmix64
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+REF_BIN = Path(__file__).resolve().parent.parent / "oracle" / "_ref" / "adb_ref_bench"
+
+
+def pair_hash_np(key, rp, sp):
+    a = (np.asarray(key, np.uint64) << np.uint64(32)) | np.asarray(rp, np.uint64)
+    b = (np.asarray(sp, np.uint64) << np.uint64(32)) | np.asarray(key, np.uint64)
+    return fmix64(a ^ fmix64(b))
+
+
+def rnd(n, key_range, seed):
+    rng = np.random.default_rng(seed)
+    return adb.tuples(rng.integers(0, key_range, size=n, dtype=np.uint64).astype(np.uint32))
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_restatements_equal_truth(oracle, seed):
+    rng = np.random.default_rng(100 + seed)
+    nR, nS = int(rng.integers(0, 3000)), int(rng.integers(0, 3000))
+    kr = int(rng.choice([3, 50, 1000, 1 << 31, 1 << 32]))
+    R, S = rnd(nR, kr, seed), rnd(nS, kr, seed + 50)
+    want = oracle.truth(R, S)
+    assert oracle.pro(R, S, 8) == want
+    assert oracle.pro(R, S, 4) == want
+    assert oracle.prh(R, S, 8) == want
+    assert oracle.npo(R, S) == want
+    assert oracle.smj(R, S) == want
+    assert oracle.shj(R, S) == want
+    assert oracle.pmj(R, S, max(1, nR // 7), max(1, nS // 5)) == want
+
+
+def test_pair_hash_matches_contract(oracle):
+    rng = np.random.default_rng(1)
+    for k, r, s in rng.integers(0, 1 << 32, size=(50, 3), dtype=np.uint64):
+        assert oracle.pair_hash(int(k), int(r), int(s)) == int(pair_hash_np(k, r, s))
+
+
+def test_golden_fixtures(oracle):
+    meta = json.loads((GOLDEN / "cases.json").read_text())
+    assert set(meta) == set(golden_cases())
+    for name, m in meta.items():
+        R = np.load(GOLDEN / f"{name}_R.npy")
+        S = np.load(GOLDEN / f"{name}_S.npy")
+        want = (m["count"], int(m["checksum"]))
+        assert oracle.truth(R, S) == want, name
+        assert oracle.pro(R, S) == want and oracle.npo(R, S) == want and oracle.smj(R, S) == want, name
+        assert oracle.shj(R, S) == want and oracle.prh(R, S) == want, name
+        # the reference's own joins, run when the fixtures were made
+        assert m["count_ref"], name
+        for algo, c in m["count_ref"].items():
+            assert c == m["count"], (name, algo)
+
+
+def test_golden_inputs_are_the_generators_output():
+    for name, (R, S) in golden_cases().items():
+        assert np.array_equal(np.load(GOLDEN / f"{name}_R.npy"), R), name
+        assert np.array_equal(np.load(GOLDEN / f"{name}_S.npy"), S), name
+
+
+@pytest.mark.parametrize("theta", [0.0, 0.5, 1.0, 1.5])
+def test_pkfk_known_answer(oracle, theta):
+    n = 20000
+    R = adb.gen_pk(n, 9)
+    S, idx = adb.gen_fk(n + 123, R, theta, 10, want_idx=True)
+    cnt, ck = oracle.truth(R, S)
+    assert cnt == n + 123
+    closed = pair_hash_np(R["key"][idx], R["payload"][idx], S["payload"]).sum(dtype=np.uint64)
+    assert ck == int(closed)
+
+
+@pytest.mark.parametrize("n", [0, 1, 5])
+def test_oracle_tiny_and_empty(oracle, n):
+    R = rnd(n, 3, 1)
+    S = rnd(7, 3, 2)
+    want = oracle.truth(R, S)
+    for f in (oracle.pro, oracle.npo, oracle.smj, oracle.shj):
+        assert f(R, S) == want
+        assert f(S, R) == oracle.truth(S, R)
+
+
+def test_all_equal_keys_count_exceeds_32_bits_formula(oracle):
+    R = adb.tuples(np.full(1500, 5, np.uint32))
+    S = adb.tuples(np.full(1700, 5, np.uint32))
+    assert oracle.truth(R, S)[0] == 1500 * 1700
+    assert oracle.npo(R, S) == oracle.truth(R, S)
+
+
+@pytest.mark.skipif(not REF_BIN.exists(), reason="the reference binary is built only where its sources are")
+@pytest.mark.parametrize("algo", ["PRO", "PRH", "RJ_st", "NPO", "NPO_st"])
+def test_reference_binary_counts(oracle, tmp_path, algo):
+    R = adb.gen_uniform(30000, 20000, 3)
+    S = adb.gen_uniform(25000, 20000, 4)
+    R.tofile(tmp_path / "R.bin")
+    S.tofile(tmp_path / "S.bin")
+    out = subprocess.run([str(REF_BIN), algo, "files", str(tmp_path / "R.bin"), str(tmp_path / "S.bin"), "4"],
+                         capture_output=True, text=True, timeout=120, check=True).stdout
+    assert json.loads(out.strip().splitlines()[-1])["count"] == oracle.truth(R, S)[0]
