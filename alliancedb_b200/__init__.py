@@ -110,6 +110,9 @@ _SIGS = {
     "adb_batch_join_device": (C.c_int, [_P, C.POINTER(C.c_uint64), _P, C.POINTER(C.c_uint64), C.c_uint32,
                                         C.c_int, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                         C.POINTER(C.c_float), _P]),
+    "adb_batch_autotune": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int)]),
+    "adb_batch_set_tuning": (C.c_int, [C.POINTER(C.c_int)]),
+    "adb_npo_join_noalloc": (C.c_int, [_P, _U64, _P, _U64, _P, _P]),
     "adb_device_alloc": (C.c_int, [C.POINTER(C.c_void_p), C.c_size_t]),
     "adb_device_free": (C.c_int, [_P]),
     "adb_host_alloc_pinned": (C.c_int, [C.POINTER(C.c_void_p), C.c_size_t]),
@@ -254,6 +257,55 @@ def batch_join_device(dR: int, r_off: np.ndarray, dS: int, s_off: np.ndarray, mo
                                      sums.ctypes.data_as(u64p), C.byref(ms), None)
     _check(st)
     return counts, sums, ms.value
+
+
+def batch_autotune(lo: int, hi: int) -> list[int]:
+    """Measure the per-window fan-out table for window sizes 2^lo .. 2^hi."""
+    out = (C.c_int * 33)()
+    _check(lib().adb_batch_autotune(lo, hi, out))
+    return list(out)
+
+
+def batch_set_tuning(bits: list[int] | None) -> None:
+    if bits is None:
+        _check(lib().adb_batch_set_tuning(None))
+    else:
+        arr = (C.c_int * 33)(*bits)
+        _check(lib().adb_batch_set_tuning(arr))
+
+
+class DeviceBuffer:
+    """Device memory from the library's allocator (freed on close / garbage collection)."""
+
+    def __init__(self, nbytes: int):
+        p = C.c_void_p()
+        _check(lib().adb_device_alloc(C.byref(p), max(int(nbytes), 16)))
+        self.ptr, self.nbytes = p.value, int(nbytes)
+
+    @classmethod
+    def from_host(cls, arr: np.ndarray) -> "DeviceBuffer":
+        arr = np.ascontiguousarray(arr)
+        d = cls(arr.nbytes)
+        if arr.nbytes:
+            _check(lib().adb_memcpy_h2d(d.ptr, arr.ctypes.data, arr.nbytes))
+        return d
+
+    def to_host(self, dtype, count: int) -> np.ndarray:
+        out = np.empty(count, dtype=dtype)
+        if out.nbytes:
+            _check(lib().adb_memcpy_d2h(out.ctypes.data, self.ptr, out.nbytes))
+        return out
+
+    def close(self):
+        if self.ptr:
+            lib().adb_device_free(self.ptr)
+            self.ptr = 0
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ---- generators (host) ----

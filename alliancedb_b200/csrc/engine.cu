@@ -19,6 +19,7 @@ namespace adb {
 int radix_set_attrs();
 int smj_set_attrs();
 int eager_set_attrs();
+int batch_set_attrs();
 
 static thread_local char g_err[512] = "";
 
@@ -106,6 +107,7 @@ Context *ctx_get(int *status) {
         int s = radix_set_attrs();
         if (s == ADB_OK) s = smj_set_attrs();
         if (s == ADB_OK) s = eager_set_attrs();
+        if (s == ADB_OK) s = batch_set_attrs();
         if (s != ADB_OK) {
             *status = s;
             delete c;

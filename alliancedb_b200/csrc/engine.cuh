@@ -53,7 +53,7 @@ struct Context {
     int device = -1;
     int num_sms = kNumSMs;
     cudaStream_t stream = nullptr;
-    cudaEvent_t ev[8] = {};
+    cudaEvent_t ev[12] = {};
     Workspace ws;
     unsigned long long *h_res = nullptr;   // pinned: [0] count [1] checksum [2] err [3] mat_n ...
     bool attrs_set = false;

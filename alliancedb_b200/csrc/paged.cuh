@@ -67,7 +67,13 @@ struct PassIn {
     const uint8_t *pcount;
     const uint32_t *plist;
     const uint64_t *pstart;   // [F1 + 1]
-    const uint32_t *uoff;     // [F1 + 1] first work unit of each input partition
+    const uint32_t *uoff;     // [F1 + 1] first work unit of each input partition (segments: of each segment)
+    // segmented flat input (batched windows): segment w is in[seg_off[w] .. seg_off[w+1]),
+    // partitioned 2^seg_bits[w] ways into output partitions seg_dbase[w] + d
+    const uint64_t *seg_off;
+    const uint8_t *seg_bits;
+    const uint32_t *seg_dbase;
+    const uint32_t *unit_pool;   // segmented input: first pool page of each unit ([G + 1])
 };
 
 struct PassArgs {
@@ -78,7 +84,10 @@ struct PassArgs {
     int G;               // CTAs per relation: flat chunks, or the bound on work units
     uint32_t pool_cap;   // pages per CTA pool
     uint32_t unit_pages; // paged input: pages per work unit
-    int paged;           // 0 = flat input, 1 = paged input
+    uint64_t unit_tuples;// segmented input: tuples per work unit
+    int paged;           // 0 = flat input, 1 = paged input, 2 = segmented flat input
+    uint32_t *seg_totals;// segmented input: [2][Dtot] pages per output partition (atomic sums)
+    uint32_t Dtot;
     uint32_t *npd;       // [2][F][G] pages per (this pass's digit, CTA)
     int *err;
 };
@@ -122,12 +131,41 @@ __device__ __forceinline__ void st16(uint64_t *dst, uint64_t a, uint64_t b) {
 // Stream position q of a tile (waiting tuples first, then the tile's tuples in
 // sorted order) lands at pos + q while q < room = 64 - pos % 64, else nxt + q.
 // kThreads threads hold kPTile / kThreads tuples each; thread d < F owns digit d.
-template <bool kPaged, int kThreads>
+// kMode: 0 flat input, 1 paged input (pass 2), 2 segmented flat input (batched windows).
+template <int kMode, int kThreads>
 __global__ void __launch_bounds__(kThreads, kThreads == 512 ? 2 : 1)
 partition_pass(PassArgs a) {
+    constexpr bool kPaged = kMode == 1;
     constexpr int kPer = kPTile / kThreads;
     extern __shared__ __align__(16) unsigned char smem[];
-    const uint32_t F = a.df.mask + 1;
+    const int relidx = blockIdx.y, g = blockIdx.x;
+    const PassIn &in = relidx ? a.in[1] : a.in[0];
+
+    // ---- this CTA's input: a flat chunk, a unit of input pages, or a unit of a segment
+    uint64_t b = 0, e = 0;        // flat / segmented: tuple range; paged: page-list range
+    uint32_t p1 = 0;              // paged: input partition; segmented: segment
+    DigitFn df = a.df;
+    if (kMode == 0) {
+        const uint64_t chunk = chunk_of(in.n, a.G);
+        b = (uint64_t)g * chunk;
+        e = min(in.n, b + chunk);
+    } else if ((uint32_t)g < in.uoff[a.F1]) {
+        uint32_t lo = 0, hi = a.F1;   // largest p with uoff[p] <= g
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (in.uoff[mid] <= (uint32_t)g) lo = mid; else hi = mid;
+        }
+        p1 = lo;
+        if (kMode == 1) {
+            b = in.pstart[p1] + (uint64_t)(g - in.uoff[p1]) * a.unit_pages;
+            e = min(in.pstart[p1 + 1], b + a.unit_pages);
+        } else {
+            b = in.seg_off[p1] + (uint64_t)(g - in.uoff[p1]) * a.unit_tuples;
+            e = min(in.seg_off[p1 + 1], b + a.unit_tuples);
+            df = DigitFn{0u, 0u, (1u << in.seg_bits[p1]) - 1u};
+        }
+    }
+    const uint32_t F = df.mask + 1;
     uint64_t *stage = reinterpret_cast<uint64_t *>(smem);
     uint64_t *carry = stage + kPTile;                                    // [F][16]
     uint32_t *toff = reinterpret_cast<uint32_t *>(carry + (size_t)F * kLineTuples);
@@ -140,32 +178,11 @@ partition_pass(PassArgs a) {
     uint32_t *pool_next = misc;        // [0]
     uint32_t *scan_tmp = misc + 4;     // [4..36)
 
-    const int relidx = blockIdx.y, g = blockIdx.x;
-    const PassIn &in = relidx ? a.in[1] : a.in[0];
     const PageSet &o = relidx ? a.out[1] : a.out[0];
-    const DigitFn df = a.df;
     const int tid = threadIdx.x;
-    uint32_t *npd = a.npd + (size_t)relidx * F * a.G;
-    const uint32_t pool_base = (uint32_t)g * a.pool_cap;
-
-    // ---- this CTA's input: a flat chunk, or a unit of input pages
-    uint64_t b = 0, e = 0;        // flat: tuple range; paged: page-list range
-    uint32_t p1 = 0;              // paged: input partition of this unit
-    if (!kPaged) {
-        const uint64_t chunk = chunk_of(in.n, a.G);
-        b = (uint64_t)g * chunk;
-        e = min(in.n, b + chunk);
-    } else if ((uint32_t)g < in.uoff[a.F1]) {
-        uint32_t lo = 0, hi = a.F1;   // largest p with uoff[p] <= g
-        while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (in.uoff[mid] <= (uint32_t)g) lo = mid; else hi = mid;
-        }
-        p1 = lo;
-        b = in.pstart[p1] + (uint64_t)(g - in.uoff[p1]) * a.unit_pages;
-        e = min(in.pstart[p1 + 1], b + a.unit_pages);
-    }
-    const uint32_t dbase = p1 * F;    // output digit = p1 * F + d
+    const uint32_t pool_base = kMode == 2 ? in.unit_pool[g] : (uint32_t)g * a.pool_cap;
+    const uint32_t pool_cap = kMode == 2 ? in.unit_pool[g + 1] - pool_base : a.pool_cap;
+    const uint32_t dbase = kMode == 2 ? in.seg_dbase[p1] : p1 * F;   // output digit = dbase + d
 
     for (uint32_t d = tid; d < F; d += kThreads) {
         pos[d] = kNone;
@@ -239,9 +256,9 @@ partition_pass(PassArgs a) {
                 if (full > room) {
                     const uint32_t need = (full - room + kPageTuples - 1) / kPageTuples;
                     uint32_t nf = atomicAdd(pool_next, need);
-                    if (nf + need > a.pool_cap) {   // cannot happen: the pool covers the input
+                    if (nf + need > pool_cap) {   // cannot happen: the pool covers the input
                         atomicExch(a.err, 3);
-                        nf = a.pool_cap - need;
+                        nf = pool_cap - need;
                     }
                     for (uint32_t k = 0; k < need; k++) {
                         o.log[pool_base + nf + k] = dbase + d;
@@ -310,7 +327,7 @@ partition_pass(PassArgs a) {
         if (c) {
             if (p == kNone) {
                 uint32_t nf = atomicAdd(pool_next, 1u);
-                if (nf + 1 > a.pool_cap) { atomicExch(a.err, 3); nf = a.pool_cap - 1; }
+                if (nf + 1 > pool_cap) { atomicExch(a.err, 3); nf = pool_cap - 1; }
                 o.log[pool_base + nf] = dbase + d;
                 p = (pool_base + nf) * kPageTuples;
             }
@@ -326,7 +343,14 @@ partition_pass(PassArgs a) {
     __syncthreads();
     for (uint32_t k = tid; k < used; k += kThreads) atomicAdd(&toff[o.log[pool_base + k] - dbase], 1u);
     __syncthreads();
-    for (uint32_t d = tid; d < F; d += kThreads) npd[(size_t)d * a.G + g] = toff[d];
+    if (kMode == 2) {
+        uint32_t *tot = a.seg_totals + (size_t)relidx * a.Dtot;
+        for (uint32_t d = tid; d < F; d += kThreads)
+            if (toff[d]) atomicAdd(&tot[dbase + d], toff[d]);
+    } else {
+        uint32_t *npd = a.npd + (size_t)relidx * F * a.G;
+        for (uint32_t d = tid; d < F; d += kThreads) npd[(size_t)d * a.G + g] = toff[d];
+    }
     if (tid == 0) o.nlog[g] = used;
 }
 

@@ -32,11 +32,11 @@ static void launch_pass(const PassArgs &a, uint32_t F, int G, bool paged, cudaSt
     const dim3 grid(G, 2);
     const size_t smem = pass_smem(F);
     if (F <= (1u << kSmallPassBits)) {
-        if (paged) partition_pass<true, 512><<<grid, 512, smem, st>>>(a);
-        else partition_pass<false, 512><<<grid, 512, smem, st>>>(a);
+        if (paged) partition_pass<1, 512><<<grid, 512, smem, st>>>(a);
+        else partition_pass<0, 512><<<grid, 512, smem, st>>>(a);
     } else {
-        if (paged) partition_pass<true, 1024><<<grid, 1024, smem, st>>>(a);
-        else partition_pass<false, 1024><<<grid, 1024, smem, st>>>(a);
+        if (paged) partition_pass<1, 1024><<<grid, 1024, smem, st>>>(a);
+        else partition_pass<0, 1024><<<grid, 1024, smem, st>>>(a);
     }
 }
 
@@ -268,6 +268,7 @@ int run_radix(Context *ctx, const DevJoin &j, bool hist_table, int bits, unsigne
     a.acc = acc; a.err = reinterpret_cast<int *>(acc + 2);
     a.F = F; a.bits = (uint32_t)bits;
     a.mat = j.mat; a.mat_n = acc + 3; a.mat_cap = j.mat_cap;
+    a.wbase = nullptr; a.wbits = nullptr; a.nwin = 0; a.wacc = nullptr;
     if (hist_table)
         radix_join_items<TableKind::Hist><<<ctx->num_sms, kJoinThreads, kJoinSmem, st>>>(a);
     else
@@ -278,13 +279,13 @@ int run_radix(Context *ctx, const DevJoin &j, bool hist_table, int bits, unsigne
 }
 
 int radix_set_attrs() {
-    ADB_CK(cudaFuncSetAttribute(partition_pass<false, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    ADB_CK(cudaFuncSetAttribute(partition_pass<0, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)pass_smem(1u << kSmallPassBits)));
-    ADB_CK(cudaFuncSetAttribute(partition_pass<true, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    ADB_CK(cudaFuncSetAttribute(partition_pass<1, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)pass_smem(1u << kSmallPassBits)));
-    ADB_CK(cudaFuncSetAttribute(partition_pass<false, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    ADB_CK(cudaFuncSetAttribute(partition_pass<0, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)pass_smem(1u << kMaxPassBits)));
-    ADB_CK(cudaFuncSetAttribute(partition_pass<true, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    ADB_CK(cudaFuncSetAttribute(partition_pass<1, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)pass_smem(1u << kMaxPassBits)));
     ADB_CK(cudaFuncSetAttribute(radix_join_items<TableKind::Chain>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJoinSmem));

@@ -193,6 +193,12 @@ struct JoinArgs {
     uint64_t *mat;                   // optional <S-key, S-payload> output
     unsigned long long *mat_n;
     uint64_t mat_cap;
+    // batched windows: partition p belongs to window w with wbase[w] <= p < wbase[w + 1];
+    // each item's count and checksum go to wacc[2w], wacc[2w + 1] (null: to acc)
+    const uint32_t *wbase;
+    const uint8_t *wbits;            // fan-out bits of each window (its in-partition hash skips them)
+    uint32_t nwin;
+    unsigned long long *wacc;
 };
 
 template <TableKind K>
@@ -227,6 +233,16 @@ radix_join_items(JoinArgs a) {
         const uint32_t item = slots[0];
         if (item >= n_items) break;
         const uint32_t p = find_part(a.items_off, F, item);
+        uint32_t win = 0, shift = a.bits;
+        if (a.wacc) {   // batched windows: the window of partition p
+            uint32_t lo = 0, hi = a.nwin;
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (a.wbase[mid] <= p) lo = mid; else hi = mid;
+            }
+            win = lo;
+            shift = a.wbits[lo];
+        }
         const uint64_t r0 = pR[p], nrp = pR[p + 1] - r0;
         const uint64_t s0 = pS[p], nsp = pS[p + 1] - s0;
         const uint32_t sch = (uint32_t)((nsp + kSPages - 1) / kSPages);
@@ -292,7 +308,7 @@ radix_join_items(JoinArgs a) {
                 const uint32_t c = pcnt[k], base = pdst[k];
                 for (uint32_t l = lane; l < c; l += 32) {
                     const uint32_t s = base + l;
-                    const uint32_t h = (tkey(tup[s]) >> a.bits) & bmask;
+                    const uint32_t h = (tkey(tup[s]) >> shift) & bmask;
                     aux[s] = (uint16_t)atomicExch(&heads[h], s + 1);
                 }
             }
@@ -302,7 +318,7 @@ radix_join_items(JoinArgs a) {
                 const uint32_t c = pcnt[k], base = pdst[k];
                 for (uint32_t l = lane; l < c; l += 32) {
                     const uint32_t s = base + l;
-                    const uint32_t h = (tkey(tup[s]) >> a.bits) & bmask;
+                    const uint32_t h = (tkey(tup[s]) >> shift) & bmask;
                     aux[s] = (uint16_t)atomicAdd(&heads[h + 1], 1u);
                 }
             }
@@ -327,7 +343,7 @@ radix_join_items(JoinArgs a) {
                 const uint32_t c = pcnt[k], base = pdst[k];
                 for (uint32_t l = lane; l < c; l += 32) {
                     const uint32_t s = base + l;
-                    const uint32_t h = (tkey(tup[s]) >> a.bits) & bmask;
+                    const uint32_t h = (tkey(tup[s]) >> shift) & bmask;
                     perm[heads[h + 1] + aux[s]] = (uint16_t)s;
                 }
             }
@@ -363,7 +379,7 @@ radix_join_items(JoinArgs a) {
                     if (lane + 32 * half >= (int)ccnt) continue;
                     const uint64_t s = half ? c1 : c0;
                     const uint32_t key = tkey(s);
-                    const uint32_t h = (key >> a.bits) & bmask;
+                    const uint32_t h = (key >> shift) & bmask;
                     uint64_t sh = 0;
                     bool have_sh = false;
                     if (K == TableKind::Chain) {
@@ -397,6 +413,10 @@ radix_join_items(JoinArgs a) {
                 }
                 c0 = n0; c1 = n1; ccnt = ncnt;
             }
+        }
+        if (a.wacc) {   // batched windows: this item's sums to its window
+            block_flush(acc, a.wacc + 2 * win, red);
+            acc = Acc();
         }
         __syncthreads();   // the next item rebuilds the table
     }

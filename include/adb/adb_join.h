@@ -161,6 +161,15 @@ int adb_batch_join_device(const adb_tuple *dR, const uint64_t *r_off, const adb_
                           const uint64_t *s_off, uint32_t n_windows, int mode,
                           uint64_t *counts, uint64_t *checksums, float *ms_device, void *stream);
 
+/* Batched mode 0 partitions window w 2^b ways, b taken from a table indexed by
+ * ceil(log2(max(|R_w|, |S_w|))).  adb_batch_autotune times b = default - 1,
+ * default, default + 1 for the window sizes 2^lo .. 2^hi on seeded windows and
+ * keeps the fastest; bits_out (33 entries, may be NULL) receives the table.
+ * adb_batch_set_tuning installs a table (33 entries, -1 = built-in rule;
+ * NULL restores the built-in rule for every size). */
+int adb_batch_autotune(int lo, int hi, int *bits_out);
+int adb_batch_set_tuning(const int *bits);
+
 /* ---------------------------------------------------------------------- */
 /* Device memory helpers for callers without a CUDA runtime of their own. */
 /* ---------------------------------------------------------------------- */
