@@ -78,6 +78,27 @@ class WindowResult(C.Structure):
     ]
 
 
+class ServeRequest(C.Structure):
+    _fields_ = [("arrival_us", C.c_uint64), ("n_r", C.c_uint32), ("n_s", C.c_uint32), ("seed", C.c_uint64)]
+
+
+class ServeResult(C.Structure):
+    _fields_ = [("count", C.c_uint64), ("checksum", C.c_uint64), ("latency_ms", C.c_float),
+                ("queue_ms", C.c_float), ("batch", C.c_uint32), ("status", C.c_int32)]
+
+
+class ServeConfig(C.Structure):
+    _fields_ = [("budget_bytes", C.c_uint64), ("max_batch", C.c_uint32), ("realtime", C.c_int32),
+                ("slots", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class ServeStats(C.Structure):
+    _fields_ = [("requests", C.c_uint64), ("tuples", C.c_uint64), ("batches", C.c_uint64),
+                ("makespan_ms", C.c_double), ("tuples_per_s", C.c_double), ("p50_ms", C.c_double),
+                ("p99_ms", C.c_double), ("p999_ms", C.c_double), ("mean_batch", C.c_double),
+                ("peak_arena_bytes", C.c_uint64), ("arena_bytes", C.c_uint64)]
+
+
 STREAM_TUPLE = np.dtype([("ts_ms", "<u8"), ("payload", "<u4"), ("key", "<u4")])
 assert STREAM_TUPLE.itemsize == C.sizeof(StreamTuple) == 16
 
@@ -111,6 +132,8 @@ _SIGS = {
                                         C.c_int, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                         C.POINTER(C.c_float), _P]),
     "adb_batch_autotune": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int)]),
+    "adb_serve_run": (C.c_int, [C.POINTER(ServeConfig), C.POINTER(ServeRequest), C.c_uint32,
+                                C.POINTER(ServeResult), C.POINTER(ServeStats)]),
     "adb_batch_set_tuning": (C.c_int, [C.POINTER(C.c_int)]),
     "adb_npo_join_noalloc": (C.c_int, [_P, _U64, _P, _U64, _P, _P]),
     "adb_device_alloc": (C.c_int, [C.POINTER(C.c_void_p), C.c_size_t]),
@@ -264,6 +287,20 @@ def batch_autotune(lo: int, hi: int) -> list[int]:
     out = (C.c_int * 33)()
     _check(lib().adb_batch_autotune(lo, hi, out))
     return list(out)
+
+
+def serve_run(requests, budget_bytes: int = 0, max_batch: int = 0, realtime: bool = True, slots: int = 0):
+    """Run the serving loop; requests = iterable of (arrival_us, n_r, n_s, seed).
+    Returns (list of ServeResult, ServeStats)."""
+    reqs = list(requests)
+    arr = (ServeRequest * max(len(reqs), 1))()
+    for i, (t, nr, ns, seed) in enumerate(reqs):
+        arr[i] = ServeRequest(int(t), int(nr), int(ns), int(seed))
+    res = (ServeResult * max(len(reqs), 1))()
+    st = ServeStats()
+    cfg = ServeConfig(int(budget_bytes), int(max_batch), 1 if realtime else 0, int(slots), 0)
+    _check(lib().adb_serve_run(C.byref(cfg), arr, len(reqs), res, C.byref(st)))
+    return [res[i] for i in range(len(reqs))], st
 
 
 def batch_set_tuning(bits: list[int] | None) -> None:

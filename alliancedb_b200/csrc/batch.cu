@@ -133,8 +133,11 @@ static int bits_for_window(uint64_t nr, uint64_t ns) {
 }
 
 // ---- mode 0: all windows in one launch sequence -----------------------------
-static int batch_join_all(Context *ctx, const uint64_t *dR, const uint64_t *r_off, const uint64_t *dS,
-                          const uint64_t *s_off, uint32_t W, uint64_t *counts, uint64_t *sums) {
+// Enqueues the whole batch on ctx->stream; the per-window sums (count, checksum
+// pairs) and the device-side error word land in the pinned host buffer h_out
+// (2 W + 8 words) once the stream reaches that point.
+int batch_launch(Context *ctx, const uint64_t *dR, const uint64_t *r_off, const uint64_t *dS, const uint64_t *s_off,
+                 uint32_t W, unsigned long long *h_out) {
     cudaStream_t st = ctx->stream;
     // host plan: per-window fan-out, partition bases, work units
     std::vector<uint8_t> bits(W);
@@ -294,18 +297,32 @@ static int batch_join_all(Context *ctx, const uint64_t *dR, const uint64_t *r_of
     ADB_CK(cudaGetLastError());
     ADB_CK(cudaEventRecord(ctx->ev[3], st));
     ctx->kernels += 14;
-    std::vector<unsigned long long> h(2 * W + 8);
-    ADB_CK(cudaMemcpyAsync(h.data(), wacc, (2 * W + 8) * 8, cudaMemcpyDeviceToHost, st));
-    ADB_CK(cudaStreamSynchronize(st));
-    if (h[2 * W + 2]) {
-        set_error("device-side check failed in the batched join (code %llu)", h[2 * W + 2]);
-        return ADB_ERR_DEVICE;
-    }
-    for (uint32_t w = 0; w < W; w++) {
-        counts[w] = h[2 * w];
-        sums[w] = h[2 * w + 1];
-    }
+    ADB_CK(cudaMemcpyAsync(h_out, wacc, (2 * W + 8) * 8, cudaMemcpyDeviceToHost, st));
     return ADB_OK;
+}
+
+static int batch_join_all(Context *ctx, const uint64_t *dR, const uint64_t *r_off, const uint64_t *dS,
+                          const uint64_t *s_off, uint32_t W, uint64_t *counts, uint64_t *sums) {
+    unsigned long long *h = nullptr;
+    ADB_CK(cudaMallocHost(&h, (2 * W + 8) * 8));
+    int s = batch_launch(ctx, dR, r_off, dS, s_off, W, h);
+    if (s == ADB_OK) {
+        cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) {
+            set_error("batched join: %s", cudaGetErrorString(e));
+            s = ADB_ERR_DEVICE;
+        } else if (h[2 * W + 2]) {
+            set_error("device-side check failed in the batched join (code %llu)", h[2 * W + 2]);
+            s = ADB_ERR_DEVICE;
+        } else {
+            for (uint32_t w = 0; w < W; w++) {
+                counts[w] = h[2 * w];
+                sums[w] = h[2 * w + 1];
+            }
+        }
+    }
+    cudaFreeHost(h);
+    return s;
 }
 
 int batch_set_attrs() {

@@ -110,4 +110,24 @@ struct Zipf {
     }
 };
 
+// ---- device generation kernels (grid-stride) ----
+static __global__ void gen_pk_kernel(uint64_t *R, uint64_t n, Perm perm) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        R[i] = tword((uint32_t)(1 + perm(i)), (uint32_t)i);
+}
+
+static __global__ void gen_fk_kernel(uint64_t *S, uint64_t nS, const uint64_t *R, uint64_t nR, double theta,
+                              uint64_t seed, uint32_t *idx_out, Perm rank_perm, Zipf z) {
+    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < nS; j += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t idx = theta > 0 ? rank_perm(z.sample(seed, j)) : uniform_below(seed, 3, j, nR);
+        S[j] = tword(tkey(R[idx]), (uint32_t)j);
+        if (idx_out) idx_out[j] = (uint32_t)idx;
+    }
+}
+
+static __global__ void gen_uniform_kernel(uint64_t *T, uint64_t n, uint64_t range, uint64_t seed) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        T[i] = tword((uint32_t)(1 + uniform_below(seed, 5, i, range)), (uint32_t)i);
+}
+
 }  // namespace adb

@@ -62,26 +62,9 @@ void Workspace::release() {
 static std::mutex g_ctx_mu;
 static Context *g_ctx[64];
 
-Context *ctx_get(int *status) {
-    int dev = 0;
-    int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
-        cudaGetLastError();
-        set_error("no CUDA device available");
-        *status = ADB_ERR_NO_DEVICE;
-        return nullptr;
-    }
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
-        cudaGetLastError();
-        set_error("cudaGetDevice failed");
-        *status = ADB_ERR_DEVICE;
-        return nullptr;
-    }
-    std::lock_guard<std::mutex> lk(g_ctx_mu);
-    if (g_ctx[dev]) {
-        *status = ADB_OK;
-        return g_ctx[dev];
-    }
+// Creates a context on the current device (stream, events, pinned result
+// words, kernel attributes); not registered as the device's default context.
+Context *ctx_create(int dev, int *status) {
     Context *c = new Context();
     c->device = dev;
     cudaDeviceProp prop;
@@ -114,7 +97,6 @@ Context *ctx_get(int *status) {
             return nullptr;
         }
     }
-    g_ctx[dev] = c;
     *status = ADB_OK;
     return c;
 fail:
@@ -122,6 +104,42 @@ fail:
     *status = ADB_ERR_DEVICE;
     delete c;
     return nullptr;
+}
+
+void ctx_destroy(Context *c) {
+    if (!c) return;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    c->ws.release();
+    for (auto &e : c->ev)
+        if (e) cudaEventDestroy(e);
+    if (c->h_res) cudaFreeHost(c->h_res);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+Context *ctx_get(int *status) {
+    int dev = 0;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        set_error("no CUDA device available");
+        *status = ADB_ERR_NO_DEVICE;
+        return nullptr;
+    }
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        set_error("cudaGetDevice failed");
+        *status = ADB_ERR_DEVICE;
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    if (g_ctx[dev]) {
+        *status = ADB_OK;
+        return g_ctx[dev];
+    }
+    Context *c = ctx_create(dev, status);
+    if (c) g_ctx[dev] = c;
+    return c;
 }
 
 // --------------------------------------------------------------------------
@@ -436,25 +454,6 @@ int adb_release_workspace(void) {
 // Generators
 // ==========================================================================
 namespace adb {
-
-__global__ void gen_pk_kernel(uint64_t *R, uint64_t n, Perm perm) {
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-        R[i] = tword((uint32_t)(1 + perm(i)), (uint32_t)i);
-}
-
-__global__ void gen_fk_kernel(uint64_t *S, uint64_t nS, const uint64_t *R, uint64_t nR, double theta,
-                              uint64_t seed, uint32_t *idx_out, Perm rank_perm, Zipf z) {
-    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < nS; j += (uint64_t)gridDim.x * blockDim.x) {
-        uint64_t idx = theta > 0 ? rank_perm(z.sample(seed, j)) : uniform_below(seed, 3, j, nR);
-        S[j] = tword(tkey(R[idx]), (uint32_t)j);
-        if (idx_out) idx_out[j] = (uint32_t)idx;
-    }
-}
-
-__global__ void gen_uniform_kernel(uint64_t *T, uint64_t n, uint64_t range, uint64_t seed) {
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-        T[i] = tword((uint32_t)(1 + uniform_below(seed, 5, i, range)), (uint32_t)i);
-}
 
 template <class F>
 static void host_parallel(uint64_t n, F f) {

@@ -63,5 +63,9 @@ struct Context {
 // The per-device context (created on first use).  Returns nullptr and sets
 // the error if no device is usable.
 Context *ctx_get(int *status);
+// A separate context on device `dev` (own stream, events and workspace), for
+// work that runs beside the default context; released with ctx_destroy.
+Context *ctx_create(int dev, int *status);
+void ctx_destroy(Context *c);
 
 }  // namespace adb

@@ -171,6 +171,53 @@ int adb_batch_autotune(int lo, int hi, int *bits_out);
 int adb_batch_set_tuning(const int *bits);
 
 /* ---------------------------------------------------------------------- */
+/* Serving: open-loop windowed-join requests with continuous batching.    */
+/* ---------------------------------------------------------------------- */
+
+/* One request: R = PK(n_r tuples, seed) and S = FK(n_s tuples drawn uniformly
+ * from R's keys, seed + 1), as adb_gen_pk / adb_gen_fk define them, generated
+ * on the device when the request is admitted.  arrival_us: offered arrival,
+ * microseconds after the run starts (requests ordered by it). */
+typedef struct adb_serve_request {
+    uint64_t arrival_us;
+    uint32_t n_r, n_s;
+    uint64_t seed;
+} adb_serve_request;
+
+typedef struct adb_serve_result {
+    uint64_t count, checksum;
+    float latency_ms;           /* completion - arrival, wall clock */
+    float queue_ms;             /* admission - arrival */
+    uint32_t batch;             /* the device batch that served it */
+    int32_t status;
+} adb_serve_result;
+
+typedef struct adb_serve_config {
+    uint64_t budget_bytes;      /* device memory for requests in flight; 0 = half of the free memory */
+    uint32_t max_batch;         /* most requests per batch; 0 = 256 */
+    int32_t realtime;           /* 1 = admit each request at its arrival time; 0 = all arrived at t = 0 */
+    uint32_t slots;             /* batches in flight at once (own stream + workspace each); 0 = 2 */
+    uint32_t reserved;
+} adb_serve_config;
+
+typedef struct adb_serve_stats {
+    uint64_t requests, tuples, batches;
+    double makespan_ms;         /* run start -> last completion */
+    double tuples_per_s;        /* input tuples of all requests / makespan */
+    double p50_ms, p99_ms, p999_ms;
+    double mean_batch;          /* requests per batch */
+    uint64_t peak_arena_bytes, arena_bytes;
+} adb_serve_stats;
+
+/* Runs the serving loop over the n requests: arrived requests are admitted
+ * while their inputs fit the device-memory budget (ADB_ERR_BUSY if one never
+ * can), batched with whatever else has arrived, and joined by the batched
+ * pipeline on one of `slots` concurrent slots.  res[i] receives request i's
+ * result; stats (may be NULL) the throughput and latency percentiles. */
+int adb_serve_run(const adb_serve_config *cfg, const adb_serve_request *req, uint32_t n,
+                  adb_serve_result *res, adb_serve_stats *stats);
+
+/* ---------------------------------------------------------------------- */
 /* Device memory helpers for callers without a CUDA runtime of their own. */
 /* ---------------------------------------------------------------------- */
 int adb_device_alloc(void **ptr, size_t bytes);

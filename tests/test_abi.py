@@ -37,7 +37,8 @@ def declared_functions():
 
 def test_headers_declare_the_entry_points():
     names = declared_functions()
-    for must in ("adb_join", "adb_join_device", "adb_stream_join", "adb_batch_join_device", "adb_npo_join_noalloc"):
+    for must in ("adb_join", "adb_join_device", "adb_stream_join", "adb_batch_join_device", "adb_npo_join_noalloc",
+                 "adb_serve_run", "adb_batch_autotune"):
         assert must in names, must
 
 
