@@ -1,0 +1,145 @@
+"""Synthetic workloads of the benchmark configurations beyond the single join.
+
+* batch   4096 independent R/S window pairs, sizes log-uniform in [2^10, 2^22]
+          per side, keys uniform over 4x the window size (match rate about
+          0.25), a quarter of the windows Zipf(0.8) over that key range; joined
+          by one launch sequence (mode 0) and by one sequence per window (mode 1)
+* serve   open-loop Poisson arrivals at 2000 requests/s, sizes log-uniform in
+          [2^12, 2^24] per side, FK relation with uniform keys, admission
+          budget 120 GB; throughput and p50 / p99 / p999 latency
+* stream  two streams of (ts, key, payload) at 1.6 M tuples/s each (Poisson
+          arrivals), keys uniform over 2^20 values materialised 4 times,
+          1000 ms tumbling windows, eager SHJ / PMJ
+
+All data is seeded and synthetic (no public dataset is involved); every
+workload generates its relations on the device from seeds unless stated.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+
+import numpy as np
+
+import alliancedb_b200 as adb
+
+
+def _logu(rng, lo, hi, n):
+    return np.floor(2.0 ** rng.uniform(lo, hi, size=n)).astype(np.uint64)
+
+
+def batch_windows(n_windows: int, lo: int, hi: int, seed: int):
+    """Device-resident batch: returns (dR, r_off, dS, s_off, keepalive)."""
+    rng = np.random.default_rng(seed)
+    nr = _logu(rng, lo, hi, n_windows)
+    ns = _logu(rng, lo, hi, n_windows)
+    zipf = rng.random(n_windows) < 0.25
+    r_off = np.concatenate([[0], np.cumsum(nr)]).astype(np.uint64)
+    s_off = np.concatenate([[0], np.cumsum(ns)]).astype(np.uint64)
+    L = adb.lib()
+    dR = adb.DeviceBuffer(int(r_off[-1]) * 8 + 16)
+    dS = adb.DeviceBuffer(int(s_off[-1]) * 8 + 16)
+    keep = [dR, dS]
+    dom_cap = int(4 * max(nr.max(), ns.max()))
+    dom = adb.DeviceBuffer(dom_cap * 8)
+    keep.append(dom)
+    for w in range(n_windows):
+        krange = int(4 * max(nr[w], ns[w]))
+        pr, ps = dR.ptr + int(r_off[w]) * 8, dS.ptr + int(s_off[w]) * 8
+        if zipf[w]:
+            # key domain 1..krange through a seeded permutation, both sides Zipf(0.8) over it
+            adb._check(L.adb_gen_pk(dom.ptr, krange, 7000 + w, 1))
+            adb._check(L.adb_gen_fk(pr, int(nr[w]), dom.ptr, krange, C.c_double(0.8), 8000 + w, None, 1))
+            adb._check(L.adb_gen_fk(ps, int(ns[w]), dom.ptr, krange, C.c_double(0.8), 9000 + w, None, 1))
+        else:
+            adb._check(L.adb_gen_uniform(pr, int(nr[w]), krange, 7000 + w, 1))
+            adb._check(L.adb_gen_uniform(ps, int(ns[w]), krange, 8000 + w, 1))
+    return dR.ptr, r_off, dS.ptr, s_off, keep
+
+
+def bench_batch(args):
+    lo, hi = 10, 22
+    dR, r_off, dS, s_off, keep = batch_windows(args.windows, lo, hi, 11)
+    tuples = int(r_off[-1] + s_off[-1])
+    table = adb.batch_autotune(lo, hi)
+    c0, k0, _ = adb.batch_join_device(dR, r_off, dS, s_off, 0)   # warm-up
+    ms0 = []
+    for _ in range(max(1, args.steps // 2)):
+        c, k, ms = adb.batch_join_device(dR, r_off, dS, s_off, 0)
+        assert np.array_equal(c, c0) and np.array_equal(k, k0)
+        ms0.append(ms)
+    c1, k1, ms1 = adb.batch_join_device(dR, r_off, dS, s_off, 1)
+    assert np.array_equal(c1, c0) and np.array_equal(k1, k0), "per-window and batched results differ"
+    best0 = float(np.median(ms0))
+    v0, v1 = tuples / (best0 / 1e3), tuples / (ms1 / 1e3)
+    return {"metric": "batched windows join input tuples/s", "value": v0, "unit": "tuples/s",
+            "higher_is_better": True, "n_gpus": 1, "data": "synthetic",
+            "config": {"workload": f"{args.windows} window pairs, sizes log-uniform [2^{lo}, 2^{hi}] per side, "
+                                   "keys uniform over 4x window size, 25% windows Zipf 0.8",
+                       "windows": args.windows, "tuples": tuples},
+            "ms_batched": best0, "ms_per_window_launches": ms1, "per_window_value": v1,
+            "speedup_batched_vs_per_window": v0 / v1, "matches": int(c0.sum()),
+            "fanout_bits_by_size_bucket": table[lo:hi + 1]}
+
+
+def bench_serve(args):
+    rng = np.random.default_rng(21)
+    n = args.requests
+    t = np.cumsum(rng.exponential(1e6 / 2000.0, size=n))
+    nr = _logu(rng, 12, 24, n)
+    ns = _logu(rng, 12, 24, n)
+    reqs = [(int(t[i]), int(nr[i]), int(ns[i]), 5000 + i) for i in range(n)]
+    adb.serve_run(reqs[:50], budget_bytes=120 << 30, max_batch=256, realtime=False)   # warm-up
+    res, st = adb.serve_run(reqs, budget_bytes=120 << 30, max_batch=256, realtime=True)
+    assert all(r.status == 0 and r.count == reqs[i][2] for i, r in enumerate(res))
+    return {"metric": "served join input tuples/s", "value": st.tuples_per_s, "unit": "tuples/s",
+            "higher_is_better": True, "n_gpus": 1, "data": "synthetic",
+            "config": {"workload": f"{n} requests, Poisson 2000 req/s, sizes log-uniform [2^12, 2^24] per side, "
+                                   "FK uniform keys, budget 120 GB", "requests": n},
+            "latency_ms": {"p50": st.p50_ms, "p99": st.p99_ms, "p999": st.p999_ms},
+            "batches": int(st.batches), "mean_batch": st.mean_batch, "makespan_ms": st.makespan_ms,
+            "offered_tuples_per_s": float((nr + ns).sum() / (t[-1] / 1e6)),
+            "peak_arena_gb": st.peak_arena_bytes / 2**30}
+
+
+def make_streams(seconds: float, rate_per_s: float, key_space: int, dup: int, seed: int):
+    rng = np.random.default_rng(seed)
+    out = []
+    for side in range(2):
+        n = int(seconds * rate_per_s)
+        n -= n % dup
+        ts = np.floor(np.cumsum(rng.exponential(1000.0 / rate_per_s, size=n))).astype(np.uint64)
+        base = rng.integers(1, key_space + 1, size=n // dup, dtype=np.uint64).astype(np.uint32)
+        keys = rng.permutation(np.tile(base, dup))
+        st = np.empty(n, dtype=adb.STREAM_TUPLE)
+        st["ts_ms"], st["key"], st["payload"] = ts, keys, np.arange(n, dtype=np.uint32)
+        out.append(st)
+    return out
+
+
+def bench_stream(args):
+    R, S = make_streams(8.0, 1.6e6, 1 << 20, 4, 31)
+    out = {"metric": "stream join input tuples/s", "unit": "tuples/s", "higher_is_better": True, "n_gpus": 1,
+           "data": "synthetic",
+           "config": {"workload": "2 streams x 1.6M tuples/s (Poisson), keys uniform over 2^20 materialised 4x, "
+                                  "1000 ms tumbling windows, micro-batches of 1 ms (1600 tuples per side)"}}
+    for algo in ("SHJ_JM_NP", "SHJ_JB_NP", "PMJ_JM_NP"):
+        p = adb.default_params(window_size=1000, batch_tuples=1600, nthreads=8, progressive_step=1)
+        adb.stream_join(algo, R[:20000], S[:20000], p)   # warm-up
+        t0 = time.perf_counter()
+        wins = adb.stream_join(algo, R, S, p)
+        dt = time.perf_counter() - t0
+        lat = np.array([w.latency_ms for w in wins])
+        out[algo] = {"tuples_per_s": (len(R) + len(S)) / dt, "windows": len(wins),
+                     "matches": int(sum(w.count for w in wins)),
+                     "last_batch_latency_ms": {"p50": float(np.percentile(lat, 50)),
+                                               "p99": float(np.percentile(lat, 99))}}
+    # offered load in real time: every micro-batch released at its timestamp
+    p = adb.default_params(window_size=1000, batch_tuples=1600, nthreads=8, realtime=1)
+    Rt, St = R[R["ts_ms"] < 3000], S[S["ts_ms"] < 3000]
+    wins = adb.stream_join("SHJ_JM_NP", Rt, St, p)
+    lat = np.array([w.latency_ms for w in wins])
+    out["SHJ_JM_NP_realtime"] = {"windows": len(wins), "window_latency_ms": {
+        "p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)), "max": float(lat.max())}}
+    out["value"] = out["SHJ_JM_NP"]["tuples_per_s"]
+    return out

@@ -195,11 +195,23 @@ def main():
     ap.add_argument("--theta", type=float, default=0.0)
     ap.add_argument("--cpu-budget", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="join", choices=["join", "batch", "serve", "stream"],
+                    help="join: one R/S pair (default, the headline); batch: 4096 windows, one launch "
+                         "sequence vs one per window; serve: open-loop requests, p50/p99/p999; "
+                         "stream: two timestamped streams in 1000 ms tumbling windows")
+    ap.add_argument("--windows", type=int, default=4096)
+    ap.add_argument("--requests", type=int, default=4000)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
     if args.impl == "reference":
         return reference_arm(args)
+    if args.workload != "join":
+        from alliancedb_b200 import workloads
+        line = {"batch": workloads.bench_batch, "serve": workloads.bench_serve,
+                "stream": workloads.bench_stream}[args.workload](args)
+        print(json.dumps(line), flush=True)
+        return
 
     import torch
     import alliancedb_b200 as adb
