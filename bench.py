@@ -144,34 +144,53 @@ def cpu_baseline_port(algo: str, n_sample: int, budget_s: float):
     return done / t_tot, reps
 
 
+REF_ALGOS = ("PRO", "PRH", "RJ_st", "NPO", "NPO_st")
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def ref_cpu(algo: str, n_sample: int, threads: int, reps: int):
+    """The reference's own join (oracle/_ref, compiled from its sources) on this
+    host: median tuples/s over `reps` calls after one warm-up, or None when the
+    reference build is absent or lacks `algo`."""
+    ref = ROOT / "oracle" / "_ref" / "adb_ref_bench"
+    if not ref.exists() or algo not in REF_ALGOS:
+        return None
+    out = subprocess.run([str(ref), algo, "gen", str(n_sample), str(threads), str(max(1, reps))], check=True,
+                         capture_output=True, text=True, timeout=600).stdout
+    d = json.loads(out.strip().splitlines()[-1])
+    if d["count"] != n_sample:
+        raise RuntimeError(f"reference join returned {d['count']} matches, expected {n_sample}")
+    return d["tuples_per_s"]
+
+
 def reference_arm(args):
-    """--impl reference: the reference's CPU join on this host."""
+    """--impl reference: the reference's CPU join on this host (rank 0 only)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    ref = ROOT / "oracle" / "_ref" / "adb_ref_bench"
-    n_sample = 1 << 24 if args.log2n >= 24 else 1 << args.log2n
-    if ref.exists():
-        threads = os.cpu_count() or 1
-        vals = []
-        for _ in range(args.warmup):
-            subprocess.run([str(ref), args.algo, str(n_sample), str(threads), "1"], check=True, capture_output=True)
-        for _ in range(args.steps):
-            out = subprocess.run([str(ref), args.algo, str(n_sample), str(threads), "1"], check=True,
-                                 capture_output=True, text=True).stdout
-            vals.append(json.loads(out.strip().splitlines()[-1])["tuples_per_s"])
-        value, kind, cores = statistics.median(vals), "reference", threads
-        sample = f"{args.algo} |R|=|S|=2^{n_sample.bit_length() - 1}, reference code, {threads} threads, join call only"
+    n_sample = 1 << min(args.log2n, 24)
+    threads = host_threads()
+    value = ref_cpu(args.algo, n_sample, threads, args.steps)
+    if value is not None:
+        kind, cores = "reference", threads
+        sample = (f"{args.algo} |R|=|S|=2^{n_sample.bit_length() - 1} PK-FK, reference code compiled from its "
+                  f"sources, {threads} threads, median of {args.steps} join calls after 1 warm-up")
     else:
         vals = []
         for _ in range(args.steps):
-            v, _ = cpu_baseline_port(args.algo, n_sample, 2.0)
+            v, _ = cpu_baseline_port(args.algo, min(n_sample, 1 << 22), 2.0)
             vals.append(v)
         value, kind, cores = statistics.median(vals), "port", 1
-        sample = f"{args.algo} |R|=|S|=2^{n_sample.bit_length() - 1}, oracle restatement, 1 thread"
+        sample = f"{args.algo} |R|=|S|=2^{min(args.log2n, 22)} PK-FK, oracle restatement, 1 thread"
     line = {"impl": "reference", "metric": "join input tuples/s", "value": value, "unit": "tuples/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u32 key/payload", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32 key/payload (integer)", "data": "synthetic",
             "config": workload_config(args),
             "cpu_baseline": {"value": value, "unit": "tuples/s", "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": "tuples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -181,7 +200,9 @@ def reference_arm(args):
 def workload_config(args):
     return {"workload": f"{args.algo} join |R|=|S|=2^{args.log2n}, R unique dense keys, S FK Zipf theta={args.theta}",
             "algo": args.algo, "r_tuples": 1 << args.log2n, "s_tuples": 1 << args.log2n, "theta": args.theta,
-            "tuple": "u32 key + u32 payload", "l2": "inputs 2x larger than L2 (no flush needed)"}
+            "tuple": "u32 key + u32 payload",
+            "l2": (f"inputs {16 << args.log2n >> 20} MiB, larger than the 126 MB L2 (no flush needed)"
+                   if (16 << args.log2n) > 126e6 else "inputs smaller than L2")}
 
 
 def main():
@@ -215,6 +236,7 @@ def main():
 
     import torch
     import alliancedb_b200 as adb
+    from alliancedb_b200.dist import max_over_ranks, sum_results
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -262,12 +284,8 @@ def main():
             assert (r.count, r.checksum) == want
         e1.record(stream)
         barrier()
-    ms = e0.elapsed_time(e1) / args.steps
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dev)
     kernels_per_step = r.kernels
-    if dist is not None:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
     value = 2 * n * world / (ms / 1e3)
 
     # ---- end to end through adb_join with pinned host buffers
@@ -291,11 +309,8 @@ def main():
         e_ms.append((time.perf_counter() - a) * 1e3)
         assert (rr.count, rr.checksum) == want
     barrier()
-    e2e_ms = statistics.median(e_ms)
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(statistics.median(e_ms), dev)
+    total = sum_results(want[0], want[1], dev)
     e2e_value = 2 * n * world / (e2e_ms / 1e3)
 
     # ---- roofline of the dominant kernel
@@ -303,7 +318,7 @@ def main():
     ph = np.array(phases).mean(axis=0)
     cands = PHASE_BYTES[fam]
     dom = max(cands, key=lambda k: ph[k])
-    kname = {("radix", 0): "paged_scatter", ("radix", 3): "radix_join_items",
+    kname = {("radix", 0): "partition_pass", ("radix", 3): "radix_join_items",
              ("npo", 0): "npo_build", ("npo", 3): "npo_probe"}[(fam, dom)]
     hbm, peak_kind = peaks()
     dom_bytes = cands[dom] * 2 * n
@@ -328,12 +343,19 @@ def main():
         "phases_ms": [float(x) for x in ph],
         "gpu_launches": kernels_per_step * args.steps,
         "clocks": clk.summary(),
-        "result": {"count": want[0], "checksum": hex(want[1])},
+        "result": {"count": total[0], "checksum": hex(total[1]), "over_ranks": world},
     }
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, reps = cpu_baseline_port(args.algo, 1 << 22, args.cpu_budget)
-        line["cpu_baseline"] = {"value": v, "unit": "tuples/s", "cores": 1, "kind": "port",
-                                "sample": f"oracle {args.algo} restatement on |R|=|S|=2^22 FK, {reps} runs"}
+        threads = host_threads()
+        v = ref_cpu(args.algo, 1 << 24, threads, 5)
+        if v is not None:
+            line["cpu_baseline"] = {"value": v, "unit": "tuples/s", "cores": threads, "kind": "reference",
+                                    "sample": f"reference {args.algo} on |R|=|S|=2^24 PK-FK, {threads} threads, "
+                                              "median of 5 join calls"}
+        else:
+            v, reps = cpu_baseline_port(args.algo, 1 << 22, args.cpu_budget)
+            line["cpu_baseline"] = {"value": v, "unit": "tuples/s", "cores": 1, "kind": "port",
+                                    "sample": f"oracle {args.algo} restatement on |R|=|S|=2^22 FK, {reps} runs"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
