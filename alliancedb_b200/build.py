@@ -77,9 +77,18 @@ def build_oracle() -> Path:
     return ORACLE_LIB
 
 
+def build_shim() -> None:
+    """oracle/_ref/adb_ref_bench_gpu: the reference-side shim (its join
+    signatures on libadb_b200.so) under the test harness; needs the
+    reference's headers, so only where its sources are present."""
+    if REF_SRC.is_dir():
+        _run(["make", "-s", "-C", str(ROOT / "oracle"), "shim", f"REF_SRC={REF_SRC}"])
+
+
 def build_all(verbose: bool = False) -> None:
     build_oracle()
     build_cuda(verbose)
+    build_shim()
 
 
 if __name__ == "__main__":

@@ -154,6 +154,7 @@ int run_paged_partition(Context *ctx, const DevJoin &j, DigitFn d1, const DigitF
     part_scan_totals<<<2, 1024, 0, st>>>(totals1, pstart1, p.F1);
     page_place<<<dim3(p.G1, 2), 1024, p.F1 * 4, st>>>(a1, a1.npd, nullptr, nullptr);
     ADB_CK(cudaGetLastError());
+    ADB_CK(cudaEventRecord(ctx->ev[1], st));   // end of pass 1 (callers may re-record)
     ctx->kernels += 5;
     if (p.passes == 1) {
         out->R = a1.out[0];
@@ -241,7 +242,7 @@ int run_radix(Context *ctx, const DevJoin &j, bool hist_table, int bits, unsigne
     const DigitFn d2{0u, b1, (1u << b2) - 1};
     PartOut po;
     ADB_TRY(run_paged_partition(ctx, j, d1, b2 ? &d2 : nullptr, &po, acc));
-    ADB_CK(cudaEventRecord(ctx->ev[1], st));
+    ADB_CK(cudaEventRecord(ctx->ev[2], st));   // phases: pass 1 | pass 2 | work list | join
 
     const uint32_t F = po.Fout;
     uint32_t *rch = ctx->ws.take<uint32_t>(F);
@@ -255,7 +256,6 @@ int run_radix(Context *ctx, const DevJoin &j, bool hist_table, int bits, unsigne
     make_items_paged<<<1, 1024, 0, st>>>(rch, sch, F, items_off, chunk_off, ctr);
     part_rchunks<<<(F + 7) / 8, 256, 0, st>>>(po.pstart, po.R.plist, po.R.pcount, F, kChunkW, chunk_off, cstart);
     ADB_CK(cudaGetLastError());
-    ADB_CK(cudaEventRecord(ctx->ev[2], st));
     ADB_CK(cudaEventRecord(ctx->ev[3], st));
 
     JoinArgs a;

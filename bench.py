@@ -45,8 +45,19 @@ sys.path.insert(0, str(ROOT))
 # algorithmic bytes per input tuple of each family (whole pipeline)
 ALG_BYTES = {"PRO": 24, "RJ_st": 24, "PRH": 24, "PRHO": 24, "NPO": 16, "NPO_st": 16,
              "m-way": 24, "m-pass": 24, "m-way+skew": 24}
-# dominant-phase index and its algorithmic bytes per input tuple
-PHASE_BYTES = {"radix": {0: 16, 3: 8}, "npo": {0: 8, 3: 8}}
+# Per family: phase index (adb_join_result.ms_phase) -> (kernel, algorithmic
+# bytes per input tuple of one launch, DRAM bytes per input tuple of one launch
+# measured by ncu on |R| = |S| = 2^24 (profiles/partition_pass_pro_2e24.md,
+# profiles/radix_join_items_pro_2e24.md), None where not captured).  The
+# traffic of a full-size launch is that figure times the launch's tuples: both
+# kernels stream every tuple once, so traffic grows in proportion.
+KERNELS = {
+    "radix": {0: ("partition_pass<0,512> (pass 1)", 16, (269997824 + 229477888) / 2**25),
+              1: ("partition_pass<1,512> (pass 2)", 16, (273354240 + 226931200) / 2**25),
+              3: ("radix_join_items<Chain>", 8, (273622528 + 4446208) / 2**25)},
+    "npo": {0: ("npo_build", 8, None), 3: ("npo_probe", 8, None)},
+    "smj": {0: ("partition_pass (all passes)", 16, None), 3: ("smj_items", 8, None)},
+}
 
 
 def peaks():
@@ -58,56 +69,66 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled every 200 ms in the timed region."""
+    """SM clocks and throttle reasons sampled through NVML every 5 ms while the
+    timed region runs (read-only queries; no setting is changed).  The GPU is
+    found by the PCI bus id of the CUDA device, so CUDA_VISIBLE_DEVICES is
+    honoured."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    @staticmethod
+    def _reasons(nv):
+        return {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "hw_power_brake_slowdown": nv.nvmlClocksEventReasonHwPowerBrakeSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
 
-    def __init__(self, gpu_index: int):
-        self.idx = gpu_index
-        self.proc = None
-        self.lines = []
+    def __init__(self, cuda_index: int, period_s: float = 0.005):
+        self.cuda_index = cuda_index
+        self.period = period_s
+        self.samples = []   # (sm_mhz, reasons bitmask)
+        self.bits = {}
+        self.max_mhz = None
+        self.error = None
+        self._stop = threading.Event()
+
+    def _handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        props = torch.cuda.get_device_properties(self.cuda_index)
+        bus = f"{props.pci_domain_id:08x}:{props.pci_bus_id:02x}:{props.pci_device_id:02x}.0"
+        return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+
+    def _run(self):
+        try:
+            nv, h = self._handle()
+            self.bits = self._reasons(nv)
+            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            while not self._stop.is_set():
+                self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM),
+                                     nv.nvmlDeviceGetCurrentClocksEventReasons(h)))
+                self._stop.wait(self.period)
+        except Exception as e:   # no NVML: the line says so instead of guessing clocks
+            self.error = f"{type(e).__name__}: {e}"
 
     def __enter__(self):
-        try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-        except OSError:
-            self.proc = None
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
+        time.sleep(0.02)
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+        self._stop.set()
+        self.t.join(timeout=5)
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for name, v in zip(["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"], f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(name)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        sm = [c for c, _ in self.samples]
+        reasons = sorted({name for _, r in self.samples for name, bit in self.bits.items() if r & bit})
+        out = {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz, "reasons": reasons,
+               "samples": len(sm), "source": "NVML every 5 ms during the timed region"}
+        if self.error:
+            out["error"] = self.error
+        return out
 
 
 def load_traffic(kernel: str):
@@ -314,16 +335,15 @@ def main():
     e2e_value = 2 * n * world / (e2e_ms / 1e3)
 
     # ---- roofline of the dominant kernel
-    fam = "npo" if args.algo.startswith("NPO") else "radix"
+    fam = "npo" if args.algo.startswith("NPO") else ("smj" if args.algo.startswith("m-") else "radix")
     ph = np.array(phases).mean(axis=0)
-    cands = PHASE_BYTES[fam]
+    cands = KERNELS[fam]
     dom = max(cands, key=lambda k: ph[k])
-    kname = {("radix", 0): "partition_pass", ("radix", 3): "radix_join_items",
-             ("npo", 0): "npo_build", ("npo", 3): "npo_probe"}[(fam, dom)]
+    kname, alg_per_tuple, traffic_per_tuple = cands[dom]
     hbm, peak_kind = peaks()
-    dom_bytes = cands[dom] * 2 * n
+    dom_bytes = alg_per_tuple * 2 * n
     achieved = dom_bytes / (ph[dom] / 1e3) / 1e9
-    traffic = load_traffic(kname)
+    traffic = traffic_per_tuple * 2 * n if traffic_per_tuple else None
     pipe_bytes = ALG_BYTES.get(args.algo, 24) * 2 * n
     pipe_gbs = pipe_bytes / (ms / 1e3) / 1e9
 
@@ -337,7 +357,9 @@ def main():
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_source": peak_kind,
                      "alg_bytes_per_launch": dom_bytes, "kernel_ms": float(ph[dom]),
-                     "traffic": traffic,
+                     "traffic": traffic, "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum "
+                                                           "per tuple at |R|=|S|=2^24, scaled to this launch"
+                                                           if traffic else None,
                      "pipeline": {"alg_bytes_per_tuple": ALG_BYTES.get(args.algo, 24), "achieved": pipe_gbs,
                                   "frac": pipe_gbs / hbm}},
         "phases_ms": [float(x) for x in ph],

@@ -91,8 +91,9 @@ typedef struct adb_join_result {
     int32_t status;             /* adb_status */
     int32_t kernels;            /* kernels this call launched */
     float ms_device;            /* device time of the join, CUDA events on the library stream */
-    float ms_phase[4];          /* device time per phase; radix: scatter, page lists + work list, -, join kernel;
-                                   NPO: build, -, -, probe */
+    float ms_phase[4];          /* device time per phase; radix: partition pass 1, pass 2 (0 with one pass),
+                                   work list, join kernel; NPO: build, -, -, probe; m-way: partitioning,
+                                   work list, -, sort + merge-join kernel */
     float ms_h2d;               /* host->device copy time (adb_join only) */
     uint64_t materialized;      /* tuples written to the materialisation buffer */
 } adb_join_result;

@@ -12,6 +12,12 @@
 //       relations from files of 8-byte {payload, key} tuples, one call
 // Prints one JSON line: algo, n_r, n_s, threads, count, ms (median), tuples_per_s.
 //
+// Built twice by oracle/Makefile: adb_ref_bench links the reference's join
+// objects; adb_ref_bench_gpu (ADB_SHIM defined) links the same calls against
+// alliancedb_b200/shim/reference_shim.cpp + libadb_b200.so instead, i.e. the
+// reference's call sites running the GPU library through the reference's
+// function signatures, and also prints the result's checksum.
+//
 // Platform utilities the reference links against (CPU pinning, NUMA queries,
 // the global thread count of hashing/utils/generator.cpp:57) are provided
 // below: identity CPU mapping over the online cores, one NUMA node.
@@ -113,18 +119,35 @@ static bool read_rel(const char *path, std::vector<tuple_t> &out) {
 
 typedef result_t *(*join_fn)(relation_t *, relation_t *, param_t);
 
+#ifdef ADB_SHIM
+#include "joins/onlinejoins.h"
+extern "C" uint64_t adb_shim_checksum(const result_t *res);
+#endif
+
+static join_fn lookup(const std::string &algo) {
+    static const struct {
+        const char *name;
+        join_fn fn;
+    } table[] = {
+        {"PRO", PRO}, {"PRH", PRH}, {"RJ_st", RJ_st}, {"NPO", NPO}, {"NPO_st", NPO_st},
+#ifdef ADB_SHIM
+        {"PRHO", PRHO}, {"SHJ_st", SHJ_st}, {"SHJ_JM_NP", SHJ_JM_NP}, {"SHJ_JB_NP", SHJ_JB_NP},
+        {"SHJ_JBCR_NP", SHJ_JBCR_NP}, {"PMJ_st", PMJ_st}, {"PMJ_JM_NP", PMJ_JM_NP}, {"PMJ_JB_NP", PMJ_JB_NP},
+        {"RPJ_st", RPJ_st},
+#endif
+    };
+    for (const auto &e : table)
+        if (algo == e.name) return e.fn;
+    return nullptr;
+}
+
 int main(int argc, char **argv) {
     if (argc < 3) {
         fprintf(stderr, "usage: %s <algo> gen <n> <threads> <reps> | <algo> files <R> <S> <threads>\n", argv[0]);
         return 2;
     }
     const std::string algo = argv[1];
-    join_fn fn = algo == "PRO"      ? PRO
-                 : algo == "PRH"    ? PRH
-                 : algo == "RJ_st"  ? RJ_st
-                 : algo == "NPO"    ? NPO
-                 : algo == "NPO_st" ? NPO_st
-                                    : nullptr;
+    join_fn fn = lookup(algo);
     if (!fn) {
         fprintf(stderr, "unsupported algorithm %s\n", algo.c_str());
         return 2;
@@ -154,6 +177,7 @@ int main(int argc, char **argv) {
     tuple_t *rt = alloc_rel(R0.size()), *st = alloc_rel(S0.size());
     std::vector<double> ms;
     int64_t count = -1;
+    uint64_t checksum = 0;
     for (int r = 0; r < reps + (reps > 1 ? 1 : 0); r++) {
         // fresh copies: PRO overwrites its inputs (parallel_radix_join.cpp:1176-1181)
         memcpy(rt, R0.data(), R0.size() * sizeof(tuple_t));
@@ -162,16 +186,23 @@ int main(int argc, char **argv) {
         const auto t0 = std::chrono::steady_clock::now();
         result_t *res = fn(&relR, &relS, p);
         const auto t1 = std::chrono::steady_clock::now();
-        count = res ? res->totalresults : -1;
+        if (!res) {
+            fprintf(stderr, "%s returned no result\n", algo.c_str());
+            return 1;
+        }
+        count = res->totalresults;
+#ifdef ADB_SHIM
+        checksum = adb_shim_checksum(res);
+#endif
         free(res);
         if (reps > 1 && r == 0) continue;   // warm-up
         ms.push_back(std::chrono::duration<double, std::milli>(t1 - t0).count());
     }
     std::sort(ms.begin(), ms.end());
     const double med = ms[ms.size() / 2];
-    printf("{\"algo\": \"%s\", \"n_r\": %zu, \"n_s\": %zu, \"threads\": %d, \"count\": %lld, \"ms\": %.3f, "
-           "\"tuples_per_s\": %.1f}\n",
-           algo.c_str(), R0.size(), S0.size(), nthreads, (long long)count, med,
+    printf("{\"algo\": \"%s\", \"n_r\": %zu, \"n_s\": %zu, \"threads\": %d, \"count\": %lld, "
+           "\"checksum\": %llu, \"ms\": %.3f, \"tuples_per_s\": %.1f}\n",
+           algo.c_str(), R0.size(), S0.size(), nthreads, (long long)count, (unsigned long long)checksum, med,
            (R0.size() + S0.size()) / (med / 1e3));
     return 0;
 }
