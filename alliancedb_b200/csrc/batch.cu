@@ -357,7 +357,8 @@ extern "C" int adb_batch_join_device(const adb_tuple *dR, const uint64_t *r_off,
         return ADB_ERR_ARG;
     }
     int s;
-    Context *ctx = ctx_get(&s);
+    CtxLock held_ = ctx_acquire(&s);
+    Context *ctx = held_.ctx;
     if (!ctx) return s;
     cudaStream_t saved = ctx->stream;
     if (stream) ctx->stream = (cudaStream_t)stream;
@@ -398,7 +399,8 @@ extern "C" int adb_batch_autotune(int lo, int hi, int *bits_out) {
         return ADB_ERR_ARG;
     }
     int s;
-    Context *ctx = ctx_get(&s);
+    CtxLock held_ = ctx_acquire(&s);
+    Context *ctx = held_.ctx;
     if (!ctx) return s;
     for (int bucket = lo; bucket <= hi; bucket++) {
         const uint64_t n = 1ull << bucket;

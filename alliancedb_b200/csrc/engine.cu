@@ -142,6 +142,13 @@ Context *ctx_get(int *status) {
     return c;
 }
 
+CtxLock ctx_acquire(int *status) {
+    CtxLock l;
+    l.ctx = ctx_get(status);
+    if (l.ctx) l.lk = std::unique_lock<std::recursive_mutex>(l.ctx->mu);
+    return l;
+}
+
 // --------------------------------------------------------------------------
 // Algorithm registry
 // --------------------------------------------------------------------------
@@ -328,7 +335,8 @@ int adb_join_device(const char *algo, const adb_tuple *dR, uint64_t nR, const ad
     if ((nR && !dR) || (nS && !dS)) { set_error("NULL relation"); return out->status = ADB_ERR_ARG; }
     int s = check_sizes(nR, nS);
     if (s) return out->status = s;
-    Context *ctx = ctx_get(&s);
+    CtxLock held_ = ctx_acquire(&s);
+    Context *ctx = held_.ctx;
     if (!ctx) return out->status = s;
     cudaStream_t saved = ctx->stream;
     if (stream) ctx->stream = (cudaStream_t)stream;
@@ -356,7 +364,8 @@ int adb_join_materialize_device(const char *algo, const adb_tuple *dR, uint64_t 
     if ((nR && !dR) || (nS && !dS) || (cap && !dOut)) { set_error("NULL pointer"); return out->status = ADB_ERR_ARG; }
     int s = check_sizes(nR, nS);
     if (s) return out->status = s;
-    Context *ctx = ctx_get(&s);
+    CtxLock held_ = ctx_acquire(&s);
+    Context *ctx = held_.ctx;
     if (!ctx) return out->status = s;
     cudaStream_t saved = ctx->stream;
     if (stream) ctx->stream = (cudaStream_t)stream;
@@ -380,7 +389,8 @@ int adb_join(const char *algo, const adb_tuple *R, uint64_t nR, const adb_tuple 
     if ((nR && !R) || (nS && !S)) { set_error("NULL relation"); return out->status = ADB_ERR_ARG; }
     int s = check_sizes(nR, nS);
     if (s) return out->status = s;
-    Context *ctx = ctx_get(&s);
+    CtxLock held_ = ctx_acquire(&s);
+    Context *ctx = held_.ctx;
     if (!ctx) return out->status = s;
     const size_t in_bytes = Workspace::need(nR + 2, 8) + Workspace::need(nS + 2, 8);
     s = ctx->ws.reserve(in_bytes + scratch_for(a, nR, nS, p, ctx->num_sms) + 4096);
@@ -416,7 +426,8 @@ int adb_stream_join(const char *algo, const adb_stream_tuple *R, uint64_t nR, co
     for (uint64_t i = 1; i < nS; i++)
         if (S[i].ts_ms < S[i - 1].ts_ms) { set_error("S is not ordered by timestamp (index %llu)", (unsigned long long)i); return ADB_ERR_ARG; }
     int s;
-    Context *ctx = ctx_get(&s);
+    CtxLock held_ = ctx_acquire(&s);
+    Context *ctx = held_.ctx;
     if (!ctx) return s;
     ctx->kernels = 0;
     return stream_join(ctx, a->fam, a->model, R, nR, S, nS, p, windows, max_windows, n_windows);
@@ -441,7 +452,8 @@ int adb_memcpy_d2h(void *dst, const void *src, size_t bytes) { ADB_CK(cudaMemcpy
 int adb_device_sync(void) { ADB_CK(cudaDeviceSynchronize()); return ADB_OK; }
 int adb_release_workspace(void) {
     int s;
-    Context *c = ctx_get(&s);
+    CtxLock held_ = ctx_acquire(&s);
+    Context *c = held_.ctx;
     if (!c) return s;
     ADB_CK(cudaStreamSynchronize(c->stream));
     c->ws.release();
@@ -481,7 +493,8 @@ int adb_gen_pk(adb_tuple *R, uint64_t n, uint64_t seed, int on_device) {
     uint64_t *w = reinterpret_cast<uint64_t *>(R);
     if (on_device) {
         int s;
-        Context *c = ctx_get(&s);
+        CtxLock held_ = ctx_acquire(&s);
+        Context *c = held_.ctx;
         if (!c) return s;
         gen_pk_kernel<<<c->num_sms * 8, 256, 0, c->stream>>>(w, n, perm);
         ADB_CK(cudaGetLastError());
@@ -502,7 +515,8 @@ int adb_gen_fk(adb_tuple *S, uint64_t nS, const adb_tuple *R, uint64_t nR, doubl
     const uint64_t *rw = reinterpret_cast<const uint64_t *>(R);
     if (on_device) {
         int s;
-        Context *c = ctx_get(&s);
+        CtxLock held_ = ctx_acquire(&s);
+        Context *c = held_.ctx;
         if (!c) return s;
         gen_fk_kernel<<<c->num_sms * 8, 256, 0, c->stream>>>(w, nS, rw, nR, theta, seed, idx, rank_perm, z);
         ADB_CK(cudaGetLastError());
@@ -522,7 +536,8 @@ int adb_gen_uniform(adb_tuple *T, uint64_t n, uint64_t key_range, uint64_t seed,
     uint64_t *w = reinterpret_cast<uint64_t *>(T);
     if (on_device) {
         int s;
-        Context *c = ctx_get(&s);
+        CtxLock held_ = ctx_acquire(&s);
+        Context *c = held_.ctx;
         if (!c) return s;
         gen_uniform_kernel<<<c->num_sms * 8, 256, 0, c->stream>>>(w, n, key_range, seed);
         ADB_CK(cudaGetLastError());

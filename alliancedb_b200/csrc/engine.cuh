@@ -5,6 +5,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "adb_common.cuh"
@@ -58,7 +59,18 @@ struct Context {
     unsigned long long *h_res = nullptr;   // pinned: [0] count [1] checksum [2] err [3] mat_n ...
     bool attrs_set = false;
     int kernels = 0;                       // kernels launched by the current call
+    std::recursive_mutex mu;               // held by the call that uses this context
 };
+
+// The per-device context, locked for the holder's scope: calls from several
+// host threads on one device are serialised, each owning the context's
+// stream, events and workspace while it runs.  (Recursive: a batched call
+// may run per-window joins on the same context.)
+struct CtxLock {
+    Context *ctx = nullptr;
+    std::unique_lock<std::recursive_mutex> lk;
+};
+CtxLock ctx_acquire(int *status);
 
 // The per-device context (created on first use).  Returns nullptr and sets
 // the error if no device is usable.

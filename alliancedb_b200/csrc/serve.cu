@@ -99,7 +99,8 @@ extern "C" int adb_serve_run(const adb_serve_config *cfg, const adb_serve_reques
         }
     }
     int s;
-    Context *c0 = ctx_get(&s);
+    CtxLock held_ = ctx_acquire(&s);
+    Context *c0 = held_.ctx;
     if (!c0) return s;
     const uint32_t max_batch = cfg->max_batch ? cfg->max_batch : 256;
     const uint32_t nslots = cfg->slots ? std::min<uint32_t>(cfg->slots, 4) : 2;

@@ -58,7 +58,7 @@ typedef enum adb_status {
     ADB_ERR_OOM = 2,         /* device or pinned-host allocation failed */
     ADB_ERR_DEVICE = 3,      /* a CUDA call failed; the message says which */
     ADB_ERR_TIMEOUT = 4,     /* a bounded device wait ran out */
-    ADB_ERR_UNSUPPORTED = 5, /* name known to the reference but not provided (see adb_algo_info) */
+    ADB_ERR_UNSUPPORTED = 5, /* name known to the reference but not provided (adb_algo_name reports which) */
     ADB_ERR_BUSY = 6,        /* admission refused: over the device-memory budget */
     ADB_ERR_NO_DEVICE = 7    /* no CUDA device, or the kernels were not built for it */
 } adb_status;

@@ -148,3 +148,25 @@ def test_golden_fixtures(algo):
         S = np.load(golden / f"{name}_S.npy")
         got = adb.join(algo, R, S, adb.default_params(batch_tuples=64, nthreads=4, progressive_step=10))
         assert (got.count, got.checksum) == (m["count"], int(m["checksum"])), name
+
+
+def test_threads_share_device_context(oracle):
+    # calls from several host threads serialise on the device's context
+    import threading
+    cases = [(adb.gen_pk(1 << 16, 40 + t), None) for t in range(4)]
+    cases = [(R, adb.gen_fk(1 << 17, R, 0.5, 50 + t)) for t, (R, _) in enumerate(cases)]
+    want = [oracle.truth(R, S) for R, S in cases]
+    got = [None] * len(cases)
+
+    def work(i):
+        algo = ("PRO", "NPO", "m-way", "PRH")[i]
+        for _ in range(3):
+            r = adb.join(algo, *cases[i])
+            got[i] = (r.count, r.checksum)
+
+    th = [threading.Thread(target=work, args=(i,)) for i in range(len(cases))]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    assert got == want
