@@ -265,7 +265,7 @@ int batch_launch(Context *ctx, const uint64_t *dR, const uint64_t *r_off, const 
     ADB_CK(cudaMemsetAsync(fill, 0, (2ull * Dt + 2) * 4, st));
     ADB_CK(cudaMemsetAsync(ctr, 0, 8, st));
     ADB_CK(cudaEventRecord(ctx->ev[0], st));
-    partition_pass<2, 1024><<<dim3(G, 2), 1024, pass_smem(1u << kMaxPassBits), st>>>(a);
+    partition_pass<2, kPassThreads><<<dim3(G, 2), kPassThreads, pass_smem(1u << kMaxPassBits, false), st>>>(a);
     ADB_CK(cudaGetLastError());
     ADB_CK(cudaEventRecord(ctx->ev[1], st));
     dscan<uint64_t>(st, tot, Dt, pstart, bsum64);
@@ -293,7 +293,7 @@ int batch_launch(Context *ctx, const uint64_t *dR, const uint64_t *r_off, const 
     ja.bits = 0;   // per-window fan-out: the kernel reads each window's bits
     ja.mat = nullptr; ja.mat_n = nullptr; ja.mat_cap = 0;
     ja.wbase = d_wbase; ja.wbits = d_bits; ja.nwin = W; ja.wacc = wacc;
-    radix_join_items<TableKind::Chain><<<ctx->num_sms, kJoinThreads, kJoinSmem, st>>>(ja);
+    radix_join_items<TableKind::Chain><<<ctx->num_sms * kJoinMinBlocks, kJoinThreads, kJoinSmem, st>>>(ja);
     ADB_CK(cudaGetLastError());
     ADB_CK(cudaEventRecord(ctx->ev[3], st));
     ctx->kernels += 14;
@@ -326,8 +326,8 @@ static int batch_join_all(Context *ctx, const uint64_t *dR, const uint64_t *r_of
 }
 
 int batch_set_attrs() {
-    ADB_CK(cudaFuncSetAttribute(partition_pass<2, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)pass_smem(1u << kMaxPassBits)));
+    ADB_CK(cudaFuncSetAttribute(partition_pass<2, kPassThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)pass_smem(1u << kMaxPassBits, false)));
     return ADB_OK;
 }
 

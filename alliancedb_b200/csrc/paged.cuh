@@ -11,12 +11,12 @@
 //   * output goes to 512-byte pages (64 tuples) taken from a per-CTA pool, a
 //     partition's pages chained through the CTA's page log, so partitions
 //     need not be contiguous and their sizes need not be known in advance;
-//   * each tile of 8192 tuples is counting-sorted by digit in shared memory;
-//     a partition's tuples then form a stream whose whole 128-byte lines are
-//     written with 16-byte stores by 8 adjacent threads; the 0-15 tuples past
-//     the last whole line wait in a per-partition line buffer in shared
-//     memory for the next tile (software write-combining, as in the
-//     reference's _optimized partitioner), so memory sees whole-line writes;
+//   * each tile of 4096 tuples is counting-sorted by digit in shared memory
+//     (the role of the reference's software write-combining buffers, its
+//     _optimized partitioner), then copied out so that each partition's
+//     tuples form one contiguous stream through its pages: warps store
+//     contiguous runs, and the partial sectors at the ends of a tile's run are
+//     completed in L2 by the stream's next tile, so DRAM sees whole lines;
 //   * pass 2 reads the pages of pass 1 in work units of up to unit_pages pages
 //     that never cross a pass-1 partition, so skewed partitions are split
 //     over many CTAs;
@@ -31,12 +31,13 @@
 namespace adb {
 
 constexpr int kPageTuples = 64;                 // 512-byte pages
-constexpr int kLineTuples = 16;                 // 128-byte lines
-constexpr int kPTile = 8192;                    // tuples per tile
-constexpr uint32_t kMaxPassBits = 9;            // <= 512 partitions per pass (1024 threads)
-constexpr uint32_t kSmallPassBits = 8;          // <= 256 partitions: 512 threads, two CTAs per SM
+constexpr int kPTile = 4096;                    // tuples per tile
+constexpr int kPassThreads = 512;               // threads per CTA of a pass
+constexpr int kPassMinBlocks = 2;               // CTAs per SM the registers are sized for
+constexpr uint32_t kMaxPassBits = 9;            // <= 512 partitions per pass
+constexpr uint32_t kSmallPassBits = 8;          // sort-merge: one pass up to 2^8 partitions
 constexpr uint32_t kMaxUnitPages = 2048;        // pass-2 work unit: <= 128K tuples
-constexpr uint32_t kMinUnitPages = 128;         // one tile
+constexpr uint32_t kMinUnitPages = kPTile / 64;  // one tile
 constexpr uint32_t kNone = 0xFFFFFFFFu;
 
 // Pages written by one pass for one relation.
@@ -97,46 +98,55 @@ __host__ __device__ __forceinline__ uint32_t flat_pool_cap(uint64_t n, int G, ui
 }
 __host__ __device__ __forceinline__ uint32_t unit_pool_cap(uint32_t F, uint32_t unit_pages) { return unit_pages + F + 1; }
 
-// Pass-2 work-unit size: about four waves of two CTAs per SM over both
+// Pass-2 work-unit size: about four waves of the resident CTAs over both
 // relations (units never cross a pass-1 partition, so there are a few more).
 __host__ __device__ __forceinline__ uint32_t unit_pages_for(uint64_t pages1_both, int num_sms) {
-    uint64_t u = pages1_both / (8ull * num_sms) + 1;
+    uint64_t u = pages1_both / (4ull * kPassMinBlocks * num_sms) + 1;
     if (u < kMinUnitPages) u = kMinUnitPages;
     if (u > kMaxUnitPages) u = kMaxUnitPages;
     return (uint32_t)u;
 }
 
-// Whole lines a tile can hold: every digit may complete one line from its
-// waiting tuples plus the tile's own 8192 tuples.
-__host__ __device__ __forceinline__ uint32_t max_tile_lines(uint32_t F) { return kPTile / kLineTuples + F; }
-
-// stage[kPTile] u64 | carry[F][16] u64 | toff[F+1] | loff[F+1] | pos[F] | nxt[F] u32 |
-// linedig[max lines] u16 | cc[F] u8 | misc
-__host__ __device__ __forceinline__ size_t pass_smem(uint32_t F) {
-    return (size_t)kPTile * 8 + (size_t)F * kLineTuples * 8 + ((size_t)F + 1) * 4 * 2 + (size_t)F * 4 * 2 +
-           (size_t)max_tile_lines(F) * 2 + (size_t)F + 256;
+// Shared memory of one pass:
+//   stage[kPTile] u64 | cnt[2][F] | toff[F] | lim[F] | b1[F] | b2[F] | npos[F] u32 | misc[48] u32
+//   | paged input only: upage[kMaxUnitPages] u32 | ucnt[kMaxUnitPages] u8
+__host__ __device__ __forceinline__ size_t pass_smem(uint32_t F, bool paged) {
+    return (size_t)kPTile * 8 + (size_t)F * 4 * 7 + 48 * 4 + (paged ? (size_t)kMaxUnitPages * 5 : 0);
 }
 
-__device__ __forceinline__ void st16(uint64_t *dst, uint64_t a, uint64_t b) {
-    *reinterpret_cast<ulonglong2 *>(dst) = make_ulonglong2(a, b);
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    return x;
 }
 
-// One pass.  Per digit d of this CTA:
-//   pos[d]  global tuple index of the next free line in the current page (a
-//           multiple of 16), or kNone when that page is full or absent;
-//   cc[d]   tuples waiting in carry[d][0..cc), stream positions 0..cc of the
-//           next tile;
-//   nxt[d]  per tile: tuple index of stream position 0 in the freshly taken
-//           pages minus the room left in the current page.
-// Stream position q of a tile (waiting tuples first, then the tile's tuples in
-// sorted order) lands at pos + q while q < room = 64 - pos % 64, else nxt + q.
-// kThreads threads hold kPTile / kThreads tuples each; thread d < F owns digit d.
-// kMode: 0 flat input, 1 paged input (pass 2), 2 segmented flat input (batched windows).
+// One pass over one input unit (a flat chunk, a unit of input pages, or a
+// unit of a segment).  Per tile of up to kPTile tuples:
+//   A  every thread ranks its tuples within their digit (shared atomics on
+//      cnt[tile parity][d]);
+//   B  warp 0 alone turns the counts into the tile's digit runs (toff), takes
+//      the pages each digit's stream needs from the CTA's pool, and advances
+//      the streams (npos = next free slot of the digit's current page, kNone
+//      when there is none);
+//   C  every thread puts its tuples into the stage, grouped by digit;
+//   D  every thread copies stage slots to their pages: slot i of digit d goes
+//      to i + b1[d] while i < lim[d] (the rest of the current page), else to
+//      i + b2[d] (the pages taken in B, consecutive in the pool).
+// Consecutive stage slots of a digit go to consecutive addresses, so warps
+// store contiguous runs; a run's partial first and last 32-byte sectors are
+// completed by the neighbouring tiles of the same stream while the line is
+// still in L2.  Three barriers per tile; the next tile's loads are in flight
+// during D.  kMode: 0 flat input, 1 paged input (pass 2), 2 segmented flat
+// input (batched windows).
 template <int kMode, int kThreads>
-__global__ void __launch_bounds__(kThreads, kThreads == 512 ? 2 : 1)
+__global__ void __launch_bounds__(kThreads, kPassMinBlocks)
 partition_pass(PassArgs a) {
     constexpr bool kPaged = kMode == 1;
     constexpr int kPer = kPTile / kThreads;
+    static_assert(kPer % 2 == 0 && kThreads % 32 == 0 && (kPTile / kPageTuples) % (kThreads / 32) == 0, "tile shape");
     extern __shared__ __align__(16) unsigned char smem[];
     const int relidx = blockIdx.y, g = blockIdx.x;
     const PassIn &in = relidx ? a.in[1] : a.in[0];
@@ -167,178 +177,176 @@ partition_pass(PassArgs a) {
     }
     const uint32_t F = df.mask + 1;
     uint64_t *stage = reinterpret_cast<uint64_t *>(smem);
-    uint64_t *carry = stage + kPTile;                                    // [F][16]
-    uint32_t *toff = reinterpret_cast<uint32_t *>(carry + (size_t)F * kLineTuples);
-    uint32_t *loff = toff + F + 1;
-    uint32_t *pos = loff + F + 1;
-    uint32_t *nxt = pos + F;
-    uint16_t *linedig = reinterpret_cast<uint16_t *>(nxt + F);           // digit of each whole line
-    uint8_t *cc = reinterpret_cast<uint8_t *>(linedig + max_tile_lines(F));
-    uint32_t *misc = reinterpret_cast<uint32_t *>((reinterpret_cast<uintptr_t>(cc + F) + 15) & ~(uintptr_t)15);
-    uint32_t *pool_next = misc;        // [0]
-    uint32_t *scan_tmp = misc + 4;     // [4..36)
+    uint32_t *cnt = reinterpret_cast<uint32_t *>(stage + kPTile);   // [2][F]
+    uint32_t *toff = cnt + 2 * F;
+    uint32_t *lim = toff + F;
+    uint32_t *b1 = lim + F;
+    uint32_t *b2 = b1 + F;
+    uint32_t *npos = b2 + F;
+    uint32_t *misc = npos + F;          // [0] pool pages taken, [1] tuples in the tile
+    uint32_t *upage = misc + 48;        // paged input: this unit's pages
+    uint8_t *ucnt = reinterpret_cast<uint8_t *>(upage + kMaxUnitPages);
 
     const PageSet &o = relidx ? a.out[1] : a.out[0];
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31;
     const uint32_t pool_base = kMode == 2 ? in.unit_pool[g] : (uint32_t)g * a.pool_cap;
     const uint32_t pool_cap = kMode == 2 ? in.unit_pool[g + 1] - pool_base : a.pool_cap;
     const uint32_t dbase = kMode == 2 ? in.seg_dbase[p1] : p1 * F;   // output digit = dbase + d
 
     for (uint32_t d = tid; d < F; d += kThreads) {
-        pos[d] = kNone;
-        cc[d] = 0;
-        toff[d] = 0;
+        cnt[d] = 0;
+        cnt[F + d] = 0;
+        npos[d] = kNone;
     }
-    if (tid == 0) *pool_next = 0;
+    if (tid == 0) misc[0] = 0;
+    if (kPaged)
+        for (uint64_t i = b + tid; i < e; i += kThreads) {
+            const uint32_t pg = in.plist[i];
+            upage[i - b] = pg;
+            ucnt[i - b] = in.pcount[pg];
+        }
     __syncthreads();
 
-    // ---- tiles: flat tiles of 8192 tuples, or 128 input pages
+    // ---- tiles: kPTile flat tuples, or kPTile / 64 input pages
     constexpr uint64_t kStep = kPaged ? (uint64_t)(kPTile / kPageTuples) : (uint64_t)kPTile;
+    const bool vec = !kPaged && ((reinterpret_cast<uintptr_t>(in.in + b) & 15) == 0);
     uint64_t w[kPer];
     uint32_t valid = 0;   // bit k: w[k] holds a tuple
     auto load_tile = [&](uint64_t t0) {
         valid = 0;
-        if (!kPaged) {
+        if (kPaged) {
+            // tuple pair k of this thread: slots 2 (tid % 32), +1 of the tile's page k * (kThreads / 32) + tid / 32
+            const uint32_t slot = 2 * (tid & 31);
+#pragma unroll
+            for (int k = 0; k < kPer / 2; k++) {
+                const uint64_t li = t0 + (uint64_t)k * (kThreads / 32) + tid / 32;
+                const uint32_t c = li < e ? ucnt[li - b] : 0u;
+                if (slot + 1 < c) {
+                    const ulonglong2 v = __ldcs(reinterpret_cast<const ulonglong2 *>(
+                        in.pages + (uint64_t)upage[li - b] * kPageTuples + slot));
+                    w[2 * k] = v.x;
+                    w[2 * k + 1] = v.y;
+                    valid |= 3u << (2 * k);
+                } else {
+                    const bool ok = slot < c;
+                    w[2 * k] = ok ? ld_stream(in.pages + (uint64_t)upage[li - b] * kPageTuples + slot) : 0;
+                    w[2 * k + 1] = 0;
+                    valid |= (ok ? 1u : 0u) << (2 * k);
+                }
+            }
+        } else if (vec) {
+#pragma unroll
+            for (int k = 0; k < kPer / 2; k++) {
+                const uint64_t i = t0 + 2 * ((uint64_t)k * kThreads + tid);
+                if (i + 1 < e) {
+                    const ulonglong2 v = __ldcs(reinterpret_cast<const ulonglong2 *>(in.in + i));
+                    w[2 * k] = v.x;
+                    w[2 * k + 1] = v.y;
+                    valid |= 3u << (2 * k);
+                } else {
+                    w[2 * k] = i < e ? ld_stream(in.in + i) : 0;
+                    w[2 * k + 1] = 0;
+                    valid |= (i < e ? 1u : 0u) << (2 * k);
+                }
+            }
+        } else {
 #pragma unroll
             for (int k = 0; k < kPer; k++) {
                 const uint64_t i = t0 + (uint64_t)k * kThreads + tid;
                 w[k] = i < e ? ld_stream(in.in + i) : 0;
                 valid |= (i < e ? 1u : 0u) << k;
             }
-        } else {
-            // tuple k of this thread: slot tid % 64 of the tile's page k * (kThreads / 64) + tid / 64
-            const uint32_t slot = tid & (kPageTuples - 1);
-            uint32_t pg[kPer];
-#pragma unroll
-            for (int k = 0; k < kPer; k++) {
-                const uint64_t li = t0 + (uint64_t)k * (kThreads / kPageTuples) + tid / kPageTuples;
-                pg[k] = li < e ? in.plist[li] : kNone;
-            }
-#pragma unroll
-            for (int k = 0; k < kPer; k++) {
-                const bool ok = pg[k] != kNone && slot < in.pcount[pg[k] == kNone ? 0 : pg[k]];
-                w[k] = ok ? ld_stream(in.pages + (uint64_t)pg[k] * kPageTuples + slot) : 0;
-                valid |= (ok ? 1u : 0u) << k;
-            }
         }
     };
-    auto room_of = [&](uint32_t p) -> uint32_t { return p == kNone ? 0u : kPageTuples - (p & (kPageTuples - 1)); };
 
     if (b < e) load_tile(b);
-    for (uint64_t t0 = b; t0 < e; t0 += kStep) {
-        // A. rank each tuple within its digit (toff[] is zero here)
-        uint32_t rk[(kPer + 1) / 2];   // two 16-bit ranks per word
+    uint32_t par = 0;
+    for (uint64_t t0 = b; t0 < e; t0 += kStep, par ^= F) {
+        uint32_t *c = cnt + par;
+        // A. rank each tuple within its digit
+        uint32_t rk[kPer / 2];   // two 16-bit ranks per word
 #pragma unroll
         for (int k = 0; k < kPer; k++) {
-            const uint32_t r = (valid >> k) & 1 ? atomicAdd(&toff[df(tkey(w[k]))], 1u) : 0u;
+            const uint32_t r = (valid >> k) & 1 ? atomicAdd(&c[df(tkey(w[k]))], 1u) : 0u;
             if (k & 1) rk[k / 2] |= r << 16; else rk[k / 2] = r;
         }
         __syncthreads();
-        // B. per digit (owner = thread d): tile offset, whole lines, new pages
-        uint32_t L = 0, c = 0, full = 0, my_toff = 0;
-        {
-            uint32_t lines = 0;
-            if (tid < (int)F) {
-                L = toff[tid];
-                c = cc[tid];
-                lines = (c + L) / kLineTuples;
-                full = lines * kLineTuples;
-            }
-            uint32_t tot;
-            const uint32_t ex = block_exclusive_scan(L | (lines << 16), scan_tmp, &tot);   // L <= 8192 < 2^16
-            if (tid < (int)F) {
-                const uint32_t d = tid;
-                my_toff = ex & 0xFFFFu;
-                toff[d] = my_toff;
-                loff[d] = ex >> 16;
-                for (uint32_t k = 0; k < lines; k++) linedig[(ex >> 16) + k] = (uint16_t)d;
-                const uint32_t room = room_of(pos[d]);
-                if (full > room) {
-                    const uint32_t need = (full - room + kPageTuples - 1) / kPageTuples;
-                    uint32_t nf = atomicAdd(pool_next, need);
-                    if (nf + need > pool_cap) {   // cannot happen: the pool covers the input
-                        atomicExch(a.err, 3);
-                        nf = pool_cap - need;
-                    }
-                    for (uint32_t k = 0; k < need; k++) {
-                        o.log[pool_base + nf + k] = dbase + d;
-                        o.pcount[pool_base + nf + k] = kPageTuples;
-                    }
-                    nxt[d] = (pool_base + nf) * kPageTuples - room;
+        // B. warp 0: digit runs of the tile, pages, stream positions
+        if (tid < 32) {
+            uint32_t run = 0, pages = 0;   // running totals over the digits done
+            const uint32_t pool0 = misc[0];
+            for (uint32_t d0 = 0; d0 < F; d0 += 32) {
+                const uint32_t d = d0 + lane;
+                uint32_t L = 0, p = kNone, room = 0, need = 0;
+                if (d < F) {
+                    L = c[d];
+                    p = npos[d];
+                    room = p == kNone ? 0u : kPageTuples - (p & (kPageTuples - 1));
+                    need = L > room ? (L - room + kPageTuples - 1) / kPageTuples : 0u;
                 }
+                const uint32_t v = L | (need << 16);   // L <= kPTile, pages per 32 digits < 2^16
+                const uint32_t inc = warp_incl_scan(v, lane);
+                const uint32_t ex = inc - v;
+                if (d < F) {
+                    const uint32_t off = run + (ex & 0xFFFFu);
+                    c[d] = 0;
+                    toff[d] = off;
+                    lim[d] = off + (L < room ? L : room);
+                    b1[d] = p - off;
+                    uint32_t np = p + L;
+                    if (need) {
+                        uint32_t first = pool0 + pages + (ex >> 16);
+                        if (first + need > pool_cap) {   // cannot happen: the pool covers the input
+                            atomicExch(a.err, 3);
+                            first = pool_cap - need;
+                        }
+                        for (uint32_t k = 0; k < need; k++) {
+                            o.log[pool_base + first + k] = dbase + d;
+                            o.pcount[pool_base + first + k] = kPageTuples;
+                        }
+                        const uint32_t nx = (pool_base + first) * kPageTuples - room;
+                        b2[d] = nx - off;
+                        np = nx + L;
+                    }
+                    if (L && (np & (kPageTuples - 1)) == 0) np = kNone;   // page exactly full
+                    npos[d] = np;
+                }
+                const uint32_t tot = __shfl_sync(0xffffffffu, inc, 31);
+                run += tot & 0xFFFFu;
+                pages += tot >> 16;
             }
-            if (tid == 0) {
-                toff[F] = tot & 0xFFFFu;
-                loff[F] = tot >> 16;
+            if (lane == 0) {
+                misc[0] = pool0 + pages;
+                misc[1] = run;
             }
         }
         __syncthreads();
-        // C. stage the tile sorted by digit
+        // C. stage the tile grouped by digit
 #pragma unroll
         for (int k = 0; k < kPer; k++)
             if ((valid >> k) & 1)
                 stage[toff[df(tkey(w[k]))] + ((rk[k / 2] >> ((k & 1) * 16)) & 0xFFFFu)] = w[k];
-        const uint64_t tnext = t0 + kStep;
+        const uint32_t tile_n = misc[1];
+        if (t0 + kStep < e) load_tile(t0 + kStep);   // in flight during D
         __syncthreads();
-        if (tnext < e) load_tile(tnext);   // prefetch: in flight during the writes
-        // D. whole lines: 8 threads per line, 16 bytes each
-        {
-            const uint32_t nlines = loff[F];
-            for (uint32_t li = tid / 8; li < nlines; li += kThreads / 8) {
-                const uint32_t d = linedig[li];
-                const uint32_t q = (li - loff[d]) * kLineTuples + (tid & 7) * 2;
-                const uint32_t cd = cc[d];
-                const uint32_t td = toff[d];
-                const uint64_t v0 = q < cd ? carry[d * kLineTuples + q] : stage[td + q - cd];
-                const uint64_t v1 = q + 1 < cd ? carry[d * kLineTuples + q + 1] : stage[td + q + 1 - cd];
-                const uint32_t p = pos[d];
-                const uint32_t dst = q < room_of(p) ? p + q : nxt[d] + q;
-                st16(o.pages + dst, v0, v1);
-            }
+        // D. stage slots to their pages
+        for (uint32_t i = tid; i < tile_n; i += kThreads) {
+            const uint64_t v = stage[i];
+            const uint32_t d = df(tkey(v));
+            const uint32_t dst = i + (i < lim[d] ? b1[d] : b2[d]);
+            o.pages[dst] = v;
         }
-        __syncthreads();
-        // E. owner: the rest of the stream (< 16 tuples) to the line buffer,
-        //    page state, and a zero counter for the next tile
-        if (tid < (int)F) {
-            const uint32_t d = tid;
-            if (L) {
-                const uint32_t total = c + L;
-                // positions [max(full, c), total) come from the stage; when
-                // full == 0 the waiting tuples [0, c) stay where they are
-                for (uint32_t q = full > c ? full : c; q < total; q++)
-                    carry[d * kLineTuples + (q - full)] = stage[my_toff + q - c];
-                if (full) {
-                    const uint32_t room = room_of(pos[d]);
-                    uint32_t np = full <= room ? pos[d] + full : nxt[d] + full;
-                    if ((np & (kPageTuples - 1)) == 0) np = kNone;   // page exactly full
-                    pos[d] = np;
-                }
-                cc[d] = (uint8_t)(total - full);
-            }
-            toff[d] = 0;
-        }
-        __syncthreads();
-    }
-    // F. flush the waiting tuples; record the fill of each digit's last page
-    if (tid < (int)F) {
-        const uint32_t d = tid;
-        const uint32_t c = cc[d];
-        uint32_t p = pos[d];
-        if (c) {
-            if (p == kNone) {
-                uint32_t nf = atomicAdd(pool_next, 1u);
-                if (nf + 1 > pool_cap) { atomicExch(a.err, 3); nf = pool_cap - 1; }
-                o.log[pool_base + nf] = dbase + d;
-                p = (pool_base + nf) * kPageTuples;
-            }
-            for (uint32_t k = 0; k < c; k++) o.pages[(uint64_t)p + k] = carry[d * kLineTuples + k];
-        }
-        if (p != kNone && ((p & (kPageTuples - 1)) || c))
-            o.pcount[p / kPageTuples] = (uint8_t)((p & (kPageTuples - 1)) + c);
+        // the next tile's A uses the other counter array and registers only;
+        // its B / C run after the next barrier, when every thread is past D
     }
     __syncthreads();
-    // G. pages per digit of this CTA (its log was written by this block)
-    const uint32_t used = *pool_next;
+    // E. fill of each digit's last page
+    for (uint32_t d = tid; d < F; d += kThreads) {
+        const uint32_t p = npos[d];
+        if (p != kNone && (p & (kPageTuples - 1))) o.pcount[p / kPageTuples] = (uint8_t)(p & (kPageTuples - 1));
+    }
+    // F. pages per digit of this CTA (its log was written by this block)
+    const uint32_t used = misc[0];
     for (uint32_t d = tid; d < F; d += kThreads) toff[d] = 0;
     __syncthreads();
     for (uint32_t k = tid; k < used; k += kThreads) atomicAdd(&toff[o.log[pool_base + k] - dbase], 1u);

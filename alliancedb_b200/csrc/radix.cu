@@ -16,36 +16,31 @@
 
 namespace adb {
 
-// CTAs of a flat pass: one per 8192-tuple tile up to the CTAs resident at once
-// (two per SM for the 512-thread kernel of fan-outs <= 256).
-static int flat_ctas(uint64_t nR, uint64_t nS, int num_sms, uint32_t F) {
+// CTAs of a flat pass: one per tile up to the CTAs resident at once.
+static int flat_ctas(uint64_t nR, uint64_t nS, int num_sms, uint32_t /*F*/) {
     const uint64_t n = nR > nS ? nR : nS;
-    const uint64_t cap = (uint64_t)num_sms * (F <= (1u << kSmallPassBits) ? 2 : 1);
+    const uint64_t cap = (uint64_t)num_sms * kPassMinBlocks;
     uint64_t g = (n + kPTile - 1) / kPTile;
     if (g < 1) g = 1;
     if (g > cap) g = cap;
     return (int)g;
 }
 
-// Launches one partition pass with the kernel variant for its fan-out.
+// Launches one partition pass (both relations: grid.y = relation).
 static void launch_pass(const PassArgs &a, uint32_t F, int G, bool paged, cudaStream_t st) {
     const dim3 grid(G, 2);
-    const size_t smem = pass_smem(F);
-    if (F <= (1u << kSmallPassBits)) {
-        if (paged) partition_pass<1, 512><<<grid, 512, smem, st>>>(a);
-        else partition_pass<0, 512><<<grid, 512, smem, st>>>(a);
-    } else {
-        if (paged) partition_pass<1, 1024><<<grid, 1024, smem, st>>>(a);
-        else partition_pass<0, 1024><<<grid, 1024, smem, st>>>(a);
-    }
+    const size_t smem = pass_smem(F, paged);
+    if (paged) partition_pass<1, kPassThreads><<<grid, kPassThreads, smem, st>>>(a);
+    else partition_pass<0, kPassThreads><<<grid, kPassThreads, smem, st>>>(a);
 }
 
 int radix_bits_for(uint64_t nR, int requested) {
     if (requested > 0) return requested > 14 ? 14 : requested;
     // one pass (<= 9 bits) leaves up to one partial page per CTA in every
-    // partition, so it aims at 8K-tuple partitions; two passes aim at 16K
-    int b = (int)ceil_log2_u64((nR + 8191) / 8192);
-    if (b > (int)kMaxPassBits) b = (int)ceil_log2_u64((nR + 16383) / 16384);
+    // partition, so it aims at half a join chunk; two passes at a full chunk
+    constexpr uint64_t kTarget = kRSlots >= 16384 ? 16384 : 8192;   // power of two <= kRSlots
+    int b = (int)ceil_log2_u64((nR + kTarget / 2 - 1) / (kTarget / 2));
+    if (b > (int)kMaxPassBits) b = (int)ceil_log2_u64((nR + kTarget - 1) / kTarget);
     if (b < 1) b = 1;
     if (b > 14) b = 14;
     return b;
@@ -269,24 +264,21 @@ int run_radix(Context *ctx, const DevJoin &j, bool hist_table, int bits, unsigne
     a.F = F; a.bits = (uint32_t)bits;
     a.mat = j.mat; a.mat_n = acc + 3; a.mat_cap = j.mat_cap;
     a.wbase = nullptr; a.wbits = nullptr; a.nwin = 0; a.wacc = nullptr;
+    const int grid = ctx->num_sms * kJoinMinBlocks;
     if (hist_table)
-        radix_join_items<TableKind::Hist><<<ctx->num_sms, kJoinThreads, kJoinSmem, st>>>(a);
+        radix_join_items<TableKind::Hist><<<grid, kJoinThreads, kJoinSmem, st>>>(a);
     else
-        radix_join_items<TableKind::Chain><<<ctx->num_sms, kJoinThreads, kJoinSmem, st>>>(a);
+        radix_join_items<TableKind::Chain><<<grid, kJoinThreads, kJoinSmem, st>>>(a);
     ADB_CK(cudaGetLastError());
     ctx->kernels += 4;
     return ADB_OK;
 }
 
 int radix_set_attrs() {
-    ADB_CK(cudaFuncSetAttribute(partition_pass<0, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)pass_smem(1u << kSmallPassBits)));
-    ADB_CK(cudaFuncSetAttribute(partition_pass<1, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)pass_smem(1u << kSmallPassBits)));
-    ADB_CK(cudaFuncSetAttribute(partition_pass<0, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)pass_smem(1u << kMaxPassBits)));
-    ADB_CK(cudaFuncSetAttribute(partition_pass<1, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)pass_smem(1u << kMaxPassBits)));
+    ADB_CK(cudaFuncSetAttribute(partition_pass<0, kPassThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)pass_smem(1u << kMaxPassBits, false)));
+    ADB_CK(cudaFuncSetAttribute(partition_pass<1, kPassThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)pass_smem(1u << kMaxPassBits, true)));
     ADB_CK(cudaFuncSetAttribute(radix_join_items<TableKind::Chain>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJoinSmem));
     ADB_CK(cudaFuncSetAttribute(radix_join_items<TableKind::Hist>,

@@ -21,13 +21,14 @@
 namespace adb {
 
 constexpr int kJoinThreads = 1024;
+constexpr int kJoinMinBlocks = 1;                          // CTAs per SM
 constexpr uint32_t kRSlots = 17408;                        // R tuples a CTA holds (136 KB)
 constexpr uint32_t kChunkW = kRSlots - kPageTuples;        // chunk weight budget
-constexpr uint32_t kMinPageW = 32;                         // weight floor of a page -> <= 545 pages per chunk
-constexpr uint32_t kRMaxPages = 560;
-constexpr uint32_t kSPages = 1024;                         // S pages per item
-constexpr uint32_t kMaxHeads = 8192;                       // Chain: bucket heads
-constexpr uint32_t kMaxHist = 2048;                        // Hist: buckets
+constexpr uint32_t kMinPageW = 32;                         // weight floor of a page
+constexpr uint32_t kRMaxPages = kChunkW / kMinPageW + 16;  // pages of one R chunk (bound)
+constexpr uint32_t kSPages = kJoinThreads;                 // S pages per item: <= 32 per warp (one per lane)
+constexpr uint32_t kMaxHeads = kRSlots >= 16384 ? 8192 : 4096;   // Chain: bucket heads (~2 slots each)
+constexpr uint32_t kMaxHist = kMaxHeads / 4;               // Hist: buckets
 
 __device__ __forceinline__ uint32_t page_weight(uint32_t cnt) {
     const uint32_t e = (cnt + 1) & ~1u;                    // slots a page occupies (16-byte copies)
@@ -129,6 +130,42 @@ __device__ __forceinline__ uint32_t find_part(const uint32_t *items_off, uint32_
     return lo;
 }
 
+// The same search by one warp, 32 probes per round: the largest i in [0, n)
+// with off[i] <= v (off non-decreasing, off[0] <= v).  Three dependent rounds
+// for 2^14 entries instead of fourteen.
+__device__ __forceinline__ uint32_t warp_find(const uint32_t *off, uint32_t n, uint32_t v, int lane) {
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const uint32_t step = (hi - lo + 31) / 32;
+        const uint32_t idx = lo + (uint32_t)lane * step;
+        const bool le = idx < hi && off[idx] <= v;
+        const uint32_t m = __ballot_sync(0xffffffffu, le);
+        lo += (31u - __clz(m)) * step;   // lane 0 always qualifies
+        hi = min(hi, lo + step);
+    }
+    return lo;
+}
+
+// Warp 0 takes the next work item: slots[0] = item, slots[1] = its partition,
+// slots[2] = the window of that partition (batched windows, else 0).
+__device__ __forceinline__ void take_item(uint32_t *work_counter, const uint32_t *items_off, uint32_t F,
+                                          uint32_t n_items, const uint32_t *wbase, uint32_t nwin,
+                                          volatile uint32_t *slots, int lane) {
+    uint32_t item = 0;
+    if (lane == 0) item = atomicAdd(work_counter, 1u);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    uint32_t p = 0, w = 0;
+    if (item < n_items) {
+        p = warp_find(items_off, F, item, lane);
+        if (wbase) w = warp_find(wbase, nwin, p, lane);
+    }
+    if (lane == 0) {
+        slots[0] = item;
+        slots[1] = p;
+        slots[2] = w;
+    }
+}
+
 // --- bulk async copy helpers (sm_90+ PTX) -----------------------------------
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
     const uint32_t a = (uint32_t)__cvta_generic_to_shared(bar);
@@ -174,7 +211,8 @@ constexpr size_t kJoinSmem = (size_t)kRSlots * 8 + (size_t)kRSlots * 2 + kXBytes
                              ((size_t)kRMaxPages + 1) * 4 * 2 + 1024;
 static_assert(((size_t)kRSlots * 10 + kXBytes + ((size_t)kRMaxPages + 1) * 8) % 8 == 0,
               "mbarrier must be 8-byte aligned");
-static_assert(kJoinSmem <= 232448, "join kernel exceeds the 227 KB shared-memory limit");
+static_assert(kJoinMinBlocks * (kJoinSmem + 1024) <= 233472, "join CTAs exceed the SM's shared memory");
+static_assert(kSPages <= 32 * (kJoinThreads / 32), "a warp's S pages are held one per lane");
 
 struct JoinArgs {
     const uint64_t *Rpages, *Spages;
@@ -202,7 +240,7 @@ struct JoinArgs {
 };
 
 template <TableKind K>
-__global__ void __launch_bounds__(kJoinThreads, 1)
+__global__ void __launch_bounds__(kJoinThreads, kJoinMinBlocks)
 radix_join_items(JoinArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint64_t *tup = reinterpret_cast<uint64_t *>(smem);
@@ -218,31 +256,23 @@ radix_join_items(JoinArgs a) {
     uint32_t *slots = reinterpret_cast<uint32_t *>(red + 64);            // [0] item, [4..36) scan scratch
 
     const uint32_t n_items = *a.n_items;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int kWarps = kJoinThreads / 32;
     if (threadIdx.x == 0) mbar_init(bar, 1);
+    if (warp == 0) take_item(a.work_counter, a.items_off, a.F, n_items, a.wacc ? a.wbase : nullptr, a.nwin, slots, lane);
     __syncthreads();
     uint32_t phase = 0;
     Acc acc;
     const uint32_t F = a.F;
     const uint64_t *pR = a.pstart, *pS = a.pstart + (F + 1);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    constexpr int kWarps = kJoinThreads / 32;
 
     while (true) {
-        if (threadIdx.x == 0) slots[0] = atomicAdd(a.work_counter, 1u);
-        __syncthreads();
+        // the item taken during the previous item's probe (or before the loop)
         const uint32_t item = slots[0];
         if (item >= n_items) break;
-        const uint32_t p = find_part(a.items_off, F, item);
-        uint32_t win = 0, shift = a.bits;
-        if (a.wacc) {   // batched windows: the window of partition p
-            uint32_t lo = 0, hi = a.nwin;
-            while (hi - lo > 1) {
-                const uint32_t mid = (lo + hi) >> 1;
-                if (a.wbase[mid] <= p) lo = mid; else hi = mid;
-            }
-            win = lo;
-            shift = a.wbits[lo];
-        }
+        const uint32_t p = slots[1];
+        const uint32_t win = slots[2];
+        const uint32_t shift = a.wacc ? a.wbits[win] : a.bits;
         const uint64_t r0 = pR[p], nrp = pR[p + 1] - r0;
         const uint64_t s0 = pS[p], nsp = pS[p + 1] - s0;
         const uint32_t sch = (uint32_t)((nsp + kSPages - 1) / kSPages);
@@ -254,6 +284,26 @@ radix_join_items(JoinArgs a) {
         const uint32_t nrpg = (uint32_t)(re - rb);
         const uint64_t sb = s0 + (uint64_t)sc * kSPages;
         const uint32_t nspg = (uint32_t)min((uint64_t)kSPages, nsp - (uint64_t)sc * kSPages);
+
+        // --- S chunk metadata and each warp's first page: issued now, used after the build.
+        //     Warp w takes pages w, w + kWarps, ...: lane i holds the id and count of
+        //     the warp's i-th page.
+        const uint32_t npw = warp < (int)nspg ? (nspg - warp + kWarps - 1) / kWarps : 0;
+        uint32_t my_pg = 0, my_cnt = 0;
+        if (lane < (int)npw) {
+            my_pg = a.Slist[sb + warp + (uint64_t)kWarps * lane];
+            my_cnt = a.Scount[my_pg];
+        }
+        auto load_page = [&](uint32_t i, uint64_t &x0, uint64_t &x1, uint32_t &cn) {
+            const uint32_t pgi = __shfl_sync(0xffffffffu, my_pg, i);
+            cn = __shfl_sync(0xffffffffu, my_cnt, i);
+            const uint64_t *Sp = a.Spages + (uint64_t)pgi * kPageTuples;
+            x0 = lane < (int)cn ? ld_stream(Sp + lane) : 0;
+            x1 = lane + 32 < (int)cn ? ld_stream(Sp + lane + 32) : 0;
+        };
+        uint64_t c0 = 0, c1 = 0;
+        uint32_t ccnt = 0;
+        if (npw) load_page(0, c0, c1, ccnt);
 
         // --- R chunk: page counts, 16-byte aligned destinations, one bulk copy per page
         uint32_t tot_slots = 0;
@@ -350,26 +400,10 @@ radix_join_items(JoinArgs a) {
             __syncthreads();
         }
 
-        // --- probe the S chunk.  Warp w takes pages w, w + 32, ...: lane i holds
-        //     the id and count of the warp's i-th page, and the tuples of the
-        //     next page are loaded before the current page is probed.
+        // --- probe the S chunk; the next page of a warp is loaded before the
+        //     current one is probed, and warp 0 first takes the next item
+        if (warp == 0) take_item(a.work_counter, a.items_off, F, n_items, a.wacc ? a.wbase : nullptr, a.nwin, slots, lane);
         {
-            const uint32_t npw = warp < (int)nspg ? (nspg - warp + kWarps - 1) / kWarps : 0;
-            uint32_t my_pg = 0, my_cnt = 0;
-            if (lane < (int)npw) {
-                my_pg = a.Slist[sb + warp + (uint64_t)kWarps * lane];
-                my_cnt = a.Scount[my_pg];
-            }
-            uint64_t c0 = 0, c1 = 0;
-            uint32_t ccnt = 0;
-            auto load_page = [&](uint32_t i, uint64_t &x0, uint64_t &x1, uint32_t &cn) {
-                const uint32_t pgi = __shfl_sync(0xffffffffu, my_pg, i);
-                cn = __shfl_sync(0xffffffffu, my_cnt, i);
-                const uint64_t *Sp = a.Spages + (uint64_t)pgi * kPageTuples;
-                x0 = lane < (int)cn ? ld_stream(Sp + lane) : 0;
-                x1 = lane + 32 < (int)cn ? ld_stream(Sp + lane + 32) : 0;
-            };
-            if (npw) load_page(0, c0, c1, ccnt);
             for (uint32_t i = 0; i < npw; i++) {
                 uint64_t n0 = 0, n1 = 0;
                 uint32_t ncnt = 0;
