@@ -34,10 +34,11 @@ constexpr uint32_t kSmjSPages = kSmjCap / kPageTuples;   // 128 pages <= 8192 tu
 constexpr uint32_t kSmjMaxPages = 272;              // weight floor 32: <= 8192 / 32 + 1 pages per chunk
 constexpr uint32_t kSmjThreads = 1024;
 
-// A | B | C tuple buffers, bucket counters, R page table, barrier and scratch.
-constexpr size_t kSmjSmem = (size_t)kSmjCap * 8 * 3 + ((size_t)(1u << kSmjBucketBits) + 4) * 4 +
-                            ((size_t)kSmjMaxPages + 1) * 4 * 2 + 1024;
+// A | B | C tuple buffers, bucket counters, R and S page tables, barrier and scratch.
+constexpr size_t kSmjSmem = (size_t)kSmjCap * 8 * 3 + ((size_t)(1u << kDualBucketBits) + 2) * 4 * 2 +
+                            ((size_t)kSmjMaxPages + 1) * 4 * 2 + ((size_t)kSmjSPages + 1) * 4 * 2 + 1024;
 static_assert(kSmjSmem <= 232448, "smj_items exceeds the 227 KB shared-memory limit");
+static_assert(kSmjMaxPages + kSmjSPages <= kSmjThreads, "one page-table entry per thread");
 
 struct SmjArgs {
     const uint64_t *Rpages, *Spages;
@@ -59,32 +60,33 @@ struct SmjArgs {
 __global__ void __launch_bounds__(kSmjThreads, 1)
 smj_items(SmjArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
-    uint64_t *A = reinterpret_cast<uint64_t *>(smem);       // sorted R chunk (bulk-copy target first)
-    uint64_t *B = A + kSmjCap;                              // compact staging
-    uint64_t *C = B + kSmjCap;                              // sorted S block
+    uint64_t *A = reinterpret_cast<uint64_t *>(smem);
+    uint64_t *B = A + kSmjCap;
+    uint64_t *C = B + kSmjCap;
     uint32_t *cnt = reinterpret_cast<uint32_t *>(C + kSmjCap);
-    uint32_t *pdst = cnt + (1u << kSmjBucketBits) + 4;
+    uint32_t *pdst = cnt + 2 * ((1u << kDualBucketBits) + 2);   // R page table
     uint32_t *pcnt = pdst + kSmjMaxPages + 1;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(pcnt + kSmjMaxPages + 1);
-    uint64_t *red = bar + 2;                                 // 64 u64
-    uint32_t *slots = reinterpret_cast<uint32_t *>(red + 64);
+    uint32_t *sdst = pcnt + kSmjMaxPages + 1;                // S page table
+    uint32_t *scnt = sdst + kSmjSPages + 1;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(scnt + kSmjSPages + 1);
+    uint64_t *red = bar + 2;                                 // 64 u64 (96 u32 of sort scratch)
+    uint32_t *slots = reinterpret_cast<uint32_t *>(red + 64);   // [0..3) next item, [4..36) scan scratch
 
     const uint32_t n_items = *a.n_items;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int kWarps = kSmjThreads / 32;
     if (threadIdx.x == 0) mbar_init(bar, 1);
+    if (warp == 0) take_item(a.work_counter, a.items_off, a.F, n_items, nullptr, 0, slots, lane);
     __syncthreads();
     uint32_t phase = 0;
     Acc acc;
     const uint32_t F = a.F;
     const uint64_t *pR = a.pstart, *pS = a.pstart + (F + 1);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    constexpr int kWarps = kSmjThreads / 32;
 
     while (true) {
-        if (threadIdx.x == 0) slots[0] = atomicAdd(a.work_counter, 1u);
-        __syncthreads();
         const uint32_t item = slots[0];
         if (item >= n_items) break;
-        const uint32_t p = find_part(a.items_off, F, item);
+        const uint32_t p = slots[1];
         const uint64_t r0 = pR[p], nrp = pR[p + 1] - r0;
         const uint64_t s0 = pS[p], nsp = pS[p + 1] - s0;
         const uint32_t sch = (uint32_t)((nsp + kSmjSPages - 1) / kSmjSPages);
@@ -97,105 +99,111 @@ smj_items(SmjArgs a) {
         const uint64_t sb = s0 + (uint64_t)sc * kSmjSPages;
         const uint32_t nspg = (uint32_t)min((uint64_t)kSmjSPages, nsp - (uint64_t)sc * kSmjSPages);
 
-        // --- R chunk -> A (bulk copies, 16-byte aligned slots per page)
-        uint32_t tot_slots = 0, nr = 0;
-        for (uint32_t base = 0; base < nrpg; base += blockDim.x) {
-            const uint32_t k = base + threadIdx.x;
-            uint32_t cnt_k = 0;
-            if (k < nrpg) cnt_k = a.Rcount[a.Rlist[rb + k]];
-            uint32_t tot;
-            const uint32_t dst = tot_slots + block_exclusive_scan((cnt_k + 1) & ~1u, slots + 4, &tot);
-            if (k < nrpg) { pdst[k] = dst; pcnt[k] = cnt_k; }
-            tot_slots += tot;
-        }
-        if (threadIdx.x == 0) {
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            mbar_expect_tx(bar, tot_slots * 8);
-        }
-        __syncthreads();
-        for (uint32_t k = threadIdx.x; k < nrpg; k += blockDim.x) {
-            const uint32_t c = pcnt[k];
-            if (c) {
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                bulk_g2s(A + pdst[k], a.Rpages + (uint64_t)a.Rlist[rb + k] * kPageTuples, ((c + 1) & ~1u) * 8, bar);
-            }
-        }
-        // --- S block -> C (compact, plain loads), overlapping the R copies
+        // --- R chunk -> A and S block -> C, one bulk copy per page, page slots
+        //     16-byte aligned (a page takes its count rounded up to even); the
+        //     pad slot behind an odd page is set to the all-ones word afterwards,
+        //     which sorts last and is cut off by count
+        uint32_t rslots, sslots, rpad, spad;
         {
-            uint32_t soff = 0;
-            for (uint32_t base = 0; base < nspg; base += blockDim.x) {
-                const uint32_t k = base + threadIdx.x;
-                uint32_t c = 0;
-                if (k < nspg) c = a.Scount[a.Slist[sb + k]];
-                uint32_t tot;
-                const uint32_t off = soff + block_exclusive_scan(c, slots + 4, &tot);
-                if (k < nspg) cnt[k] = off;            // page offsets (cnt is free until the sorts)
-                soff += tot;
+            const uint32_t k = threadIdx.x;   // one page per thread: R pages, then S pages
+            const bool isr = k < nrpg, iss = !isr && k < nrpg + nspg;
+            uint32_t c = 0;
+            if (isr) c = a.Rcount[a.Rlist[rb + k]];
+            else if (iss) c = a.Scount[a.Slist[sb + (k - nrpg)]];
+            const uint32_t e = (c + 1) & ~1u;
+            uint32_t tot;
+            const uint32_t ex = block_exclusive_scan(isr ? e : (e << 16), slots + 4, &tot);   // R | S << 16
+            rslots = tot & 0xFFFFu;
+            sslots = tot >> 16;
+            if (isr) { pdst[k] = ex & 0xFFFFu; pcnt[k] = c; }
+            if (iss) { sdst[k - nrpg] = (ex >> 16); scnt[k - nrpg] = c; }
+            if (threadIdx.x == 0) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                mbar_expect_tx(bar, (rslots + sslots) * 8);
             }
-            __syncthreads();
-            for (uint32_t k = warp; k < nspg; k += kWarps) {
-                const uint32_t pg = a.Slist[sb + k];
-                const uint32_t c = a.Scount[pg];
-                const uint32_t off = cnt[k];
-                const uint64_t *src = a.Spages + (uint64_t)pg * kPageTuples;
-                for (uint32_t l = lane; l < c; l += 32) C[off + l] = ld_stream(src + l);
+            rpad = __syncthreads_count(isr && (c & 1));
+            spad = __syncthreads_count(iss && (c & 1));
+        }
+        for (uint32_t k = threadIdx.x; k < nrpg + nspg; k += blockDim.x) {
+            const bool isr = k < nrpg;
+            const uint32_t kk = isr ? k : k - nrpg;
+            const uint32_t c = isr ? pcnt[kk] : scnt[kk];
+            if (c) {
+                const uint32_t pg = isr ? a.Rlist[rb + kk] : a.Slist[sb + kk];
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                bulk_g2s(isr ? A + pdst[kk] : C + sdst[kk], (isr ? a.Rpages : a.Spages) + (uint64_t)pg * kPageTuples,
+                         ((c + 1) & ~1u) * 8, bar);
             }
-            if (threadIdx.x == 0) slots[1] = soff;
         }
         if (!mbar_wait(bar, phase)) atomicExch(a.err, 1);
         phase ^= 1;
         __syncthreads();
-        const uint32_t ns = slots[1];
-        // compact R: A (page slots) -> B
-        {
-            uint32_t roff = 0;
-            for (uint32_t base = 0; base < nrpg; base += blockDim.x) {
-                const uint32_t k = base + threadIdx.x;
-                const uint32_t c = k < nrpg ? pcnt[k] : 0u;
-                uint32_t tot;
-                const uint32_t off = roff + block_exclusive_scan(c, slots + 4, &tot);
-                if (k < nrpg) cnt[k] = off;
-                roff += tot;
-            }
-            nr = roff;
-            __syncthreads();
-            for (uint32_t k = warp; k < nrpg; k += kWarps) {
-                const uint32_t c = pcnt[k], src = pdst[k], dst = cnt[k];
-                for (uint32_t l = lane; l < c; l += 32) B[dst + l] = A[src + l];
-            }
-            __syncthreads();
+        for (uint32_t k = threadIdx.x; k < nrpg + nspg; k += blockDim.x) {
+            const bool isr = k < nrpg;
+            const uint32_t kk = isr ? k : k - nrpg;
+            const uint32_t c = isr ? pcnt[kk] : scnt[kk];
+            if (c & 1) (isr ? A + pdst[kk] : C + sdst[kk])[c] = ~0ULL;
         }
-        chunk_sort(B, nr, A, cnt, reinterpret_cast<uint32_t *>(red));   // sorted R in A
-        chunk_sort(C, ns, B, cnt, reinterpret_cast<uint32_t *>(red));   // sorted S in B
+        __syncthreads();
+        // sorted R (+ pads) in B, sorted S (+ pads) in A; the pads are the last
+        // words of each run and a real all-ones tuple is the same word, so
+        // dropping as many words as there are pads is exact
+        const DualSort ds = dual_chunk_sort(A, rslots, B, C, sslots, A, cnt, reinterpret_cast<uint32_t *>(red));
+        const uint32_t nr = rslots - rpad, ns = sslots - spad;
+        const uint64_t *Rs = B, *Ss = A;
 
-        // --- merge-path join of A (R, nr) and B (S, ns); R first on equal keys
-        {
+        // --- merge-join of the sorted runs; warp 0 first takes the next item
+        if (warp == 0) take_item(a.work_counter, a.items_off, F, n_items, nullptr, 0, slots, lane);
+        auto emit = [&](uint64_t s, uint64_t r, uint64_t &sh, bool &have) {
+            const uint32_t key = tkey(s);
+            if (!have) { sh = s_half(key, tpay(s)); have = true; }
+            acc.count++;
+            acc.sum += pair_hash_pre(key, tpay(r), sh);
+            if (a.mat) {
+                const unsigned long long m = atomicAdd(a.mat_n, 1ull);
+                if (m < a.mat_cap) a.mat[m] = s;
+            }
+        };
+        // all-ones words beyond the pads: real tuples with key 0xFFFFFFFF
+        const bool ones = !ds.bitonic && (rslots - (ds.nb ? cnt[ds.nb - 1] : 0u) != rpad ||
+                                          sslots - (ds.nb ? cnt[2 * ds.nb] : 0u) != spad);
+        if (!ds.bitonic && !ds.max_key && !ones) {
+            // both runs are ordered by the same buckets: S bucket d meets R bucket
+            // d, whose sorted range [cnt[d - 1], cnt[d]) holds every R tuple that
+            // can have the S tuple's key; no key is 0xFFFFFFFF, so no pad matches
+            const uint32_t *cx = cnt;
+            for (uint32_t j = threadIdx.x; j < ns; j += blockDim.x) {
+                const uint64_t s = Ss[j];
+                const uint32_t key = tkey(s);
+                const uint32_t d = ds.bucket(s);
+                uint64_t sh = 0;
+                bool have = false;
+                for (uint32_t t = d ? cx[d - 1] : 0u, e = cx[d]; t < e; t++) {
+                    const uint64_t r = Rs[t];
+                    if (tkey(r) > key) break;
+                    if (tkey(r) == key) emit(s, r, sh, have);
+                }
+            }
+        } else {
+            // merge path over the whole runs; R first on equal keys
             const uint32_t total = nr + ns;
             const uint32_t L = (total + blockDim.x - 1) / blockDim.x;
             const uint32_t k0 = min(total, threadIdx.x * L), k1 = min(total, k0 + L);
             uint32_t lo = k0 > ns ? k0 - ns : 0u, hi = k0 < nr ? k0 : nr;
             while (lo < hi) {   // number of R tuples among the first k0 merged
                 const uint32_t mid = (lo + hi) >> 1;
-                if (tkey(A[mid]) <= tkey(B[k0 - mid - 1])) lo = mid + 1; else hi = mid;
+                if (tkey(Rs[mid]) <= tkey(Ss[k0 - mid - 1])) lo = mid + 1; else hi = mid;
             }
             uint32_t i = lo, j = k0 - lo;
             for (uint32_t k = k0; k < k1; k++) {
-                if (j >= ns || (i < nr && tkey(A[i]) <= tkey(B[j]))) {
+                if (j >= ns || (i < nr && tkey(Rs[i]) <= tkey(Ss[j]))) {
                     i++;
                 } else {
-                    const uint64_t s = B[j];
+                    const uint64_t s = Ss[j];
                     const uint32_t key = tkey(s);
                     uint64_t sh = 0;
                     bool have = false;
-                    for (int t = (int)i - 1; t >= 0 && tkey(A[t]) == key; t--) {
-                        if (!have) { sh = s_half(key, tpay(s)); have = true; }
-                        acc.count++;
-                        acc.sum += pair_hash_pre(key, tpay(A[t]), sh);
-                        if (a.mat) {
-                            const unsigned long long m = atomicAdd(a.mat_n, 1ull);
-                            if (m < a.mat_cap) a.mat[m] = s;
-                        }
-                    }
+                    for (int t = (int)i - 1; t >= 0 && tkey(Rs[t]) == key; t--) emit(s, Rs[t], sh, have);
                     j++;
                 }
             }

@@ -15,16 +15,49 @@ namespace adb {
 
 constexpr uint32_t kSmjBucketBits = 12;
 
-// Sorts src[0..n) by key into dst (both shared memory).  cnt holds 2^12 + 1
-// counters; red holds 64 scratch words.  All threads call it.
+// Bitonic sort of dst[0..n) on the whole 64-bit word, padded to a power of
+// two with all-ones words (which sort last); dst must hold that many words.
+__device__ __forceinline__ void bitonic_words(uint64_t *dst, uint32_t n) {
+    uint32_t m = 1;
+    while (m < n) m <<= 1;
+    for (uint32_t i = n + threadIdx.x; i < m; i += blockDim.x) dst[i] = ~0ULL;
+    __syncthreads();
+    for (uint32_t k = 2; k <= m; k <<= 1) {
+        for (uint32_t jj = k >> 1; jj > 0; jj >>= 1) {
+            for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+                const uint32_t l = i ^ jj;
+                if (l > i) {
+                    const uint64_t x = dst[i], y = dst[l];
+                    const bool up = (i & k) == 0;
+                    if ((x > y) == up) { dst[i] = y; dst[l] = x; }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Sorts src[0..n) into dst (both shared memory, dst with room for n rounded
+// up to a power of two) by key; tuples with key 0xFFFFFFFF are also ordered
+// by payload, so all-ones words come last.  cnt holds 2^12 + 2 counters; red
+// holds 64 scratch words.  All threads call it.
+//
+// MSD counting sort on the (at most) 12 highest key bits that differ within
+// the chunk, all-ones words in a bucket of their own behind the rest (they
+// pad callers' page slots, so they are kept out of the bit analysis); then an
+// insertion sort inside each bucket when the buckets are wider than one key.
+// A bucket of more than 128 tuples that needs sorting makes the whole chunk
+// take the bitonic path instead.
 __device__ __forceinline__ void chunk_sort(const uint64_t *src, uint32_t n, uint64_t *dst, uint32_t *cnt, uint32_t *red) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    // key bits that differ within the chunk
+    // key bits that differ within the chunk (all-ones words left out)
     uint32_t a = 0xFFFFFFFFu, o = 0;
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-        const uint32_t k = tkey(src[i]);
-        a &= k;
-        o |= k;
+        const uint64_t v = src[i];
+        if (v != ~0ULL) {
+            a &= tkey(v);
+            o |= tkey(v);
+        }
     }
 #pragma unroll
     for (int s = 16; s > 0; s >>= 1) {
@@ -36,24 +69,20 @@ __device__ __forceinline__ void chunk_sort(const uint64_t *src, uint32_t n, uint
     a = 0xFFFFFFFFu;
     o = 0;
     for (int w = 0; w < (int)(blockDim.x >> 5); w++) { a &= red[w]; o |= red[32 + w]; }
-    const uint32_t vary = a ^ o;
     __syncthreads();
-    if (vary == 0) {   // one key value: already sorted
-        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
-        __syncthreads();
-        return;
-    }
-    const uint32_t hi = 31 - __clz(vary);
-    const uint32_t nbits = hi + 1 < kSmjBucketBits ? hi + 1 : kSmjBucketBits;
-    const uint32_t shift = hi + 1 - nbits;
-    const uint32_t nb = 1u << nbits, bmask = nb - 1;
-    for (uint32_t d = threadIdx.x; d < nb; d += blockDim.x) cnt[d] = 0;
+    const uint32_t vary = (a & ~o) ? 0u : a ^ o;   // a & ~o != 0: no word counted (a stays all ones)
+    const uint32_t hi = vary ? 31 - __clz(vary) : 0u;
+    const uint32_t nbits = vary == 0 ? 0u : (hi + 1 < kSmjBucketBits ? hi + 1 : kSmjBucketBits);
+    const uint32_t shift = vary == 0 ? 0u : hi + 1 - nbits;
+    const uint32_t nb = 1u << nbits, bmask = nb - 1;   // bucket nb: all-ones words
+    auto bucket = [&](uint64_t v) { return v == ~0ULL ? nb : (tkey(v) >> shift) & bmask; };
+    for (uint32_t d = threadIdx.x; d <= nb; d += blockDim.x) cnt[d] = 0;
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) atomicAdd(&cnt[(tkey(src[i]) >> shift) & bmask], 1u);
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) atomicAdd(&cnt[bucket(src[i])], 1u);
     __syncthreads();
     {   // exclusive scan of the bucket counts, contiguous buckets per thread
-        const uint32_t per = (nb + blockDim.x - 1) / blockDim.x;
-        const uint32_t d0 = threadIdx.x * per, d1 = min(nb, d0 + per);
+        const uint32_t per = (nb + 1 + blockDim.x - 1) / blockDim.x;
+        const uint32_t d0 = threadIdx.x * per, d1 = min(nb + 1, d0 + per);
         uint32_t loc = 0;
         for (uint32_t d = d0; d < d1; d++) loc += cnt[d];
         uint32_t tot;
@@ -67,52 +96,165 @@ __device__ __forceinline__ void chunk_sort(const uint64_t *src, uint32_t n, uint
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
         const uint64_t v = src[i];
-        dst[atomicAdd(&cnt[(tkey(v) >> shift) & bmask], 1u)] = v;
+        dst[atomicAdd(&cnt[bucket(v)], 1u)] = v;
     }
     __syncthreads();
-    // cnt[d] is now the end of bucket d.  Buckets of more than 128 tuples
-    // (keys clustered below the bucket bits) would make the insertion sort
-    // quadratic: then the whole chunk is bitonic-sorted on the 64-bit word
-    // instead, padded with all-ones words that sort last.
-    if (shift) {
-        int big = 0;
-        for (uint32_t d = threadIdx.x; d < nb; d += blockDim.x)
-            if (cnt[d] - (d ? cnt[d - 1] : 0u) > 128) big = 1;
-        if (__syncthreads_or(big)) {
-            uint32_t m = 1;
-            while (m < n) m <<= 1;
-            for (uint32_t i = n + threadIdx.x; i < m; i += blockDim.x) dst[i] = ~0ULL;
-            __syncthreads();
-            for (uint32_t k = 2; k <= m; k <<= 1) {
-                for (uint32_t jj = k >> 1; jj > 0; jj >>= 1) {
-                    for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
-                        const uint32_t l = i ^ jj;
-                        if (l > i) {
-                            const uint64_t x = dst[i], y = dst[l];
-                            const bool up = (i & k) == 0;
-                            if ((x > y) == up) { dst[i] = y; dst[l] = x; }
-                        }
-                    }
-                    __syncthreads();
-                }
+    // cnt[d] is now the end of bucket d.  With shift == 0 a bucket is one key
+    // value: only the bucket of key 0xFFFFFFFF (the last one, if the chunk's
+    // common bits are all ones) needs its payloads ordered.  With shift > 0
+    // every bucket is insertion-sorted by whole word.  The all-ones bucket is
+    // one word value.
+    const uint32_t d_first = shift == 0 ? ((a | bmask) == 0xFFFFFFFFu ? bmask : nb) : 0u;
+    int big = 0;
+    for (uint32_t d = d_first + threadIdx.x; d < nb; d += blockDim.x)
+        if (cnt[d] - (d ? cnt[d - 1] : 0u) > 128) big = 1;
+    if (__syncthreads_or(big)) {
+        bitonic_words(dst, n);
+        return;
+    }
+    for (uint32_t d = d_first + threadIdx.x; d < nb; d += blockDim.x) {
+        const uint32_t b = d ? cnt[d - 1] : 0u, e = cnt[d];
+        for (uint32_t i = b + 1; i < e; i++) {
+            const uint64_t v = dst[i];
+            uint32_t j = i;
+            while (j > b && dst[j - 1] > v) {
+                dst[j] = dst[j - 1];
+                j--;
             }
-            return;
+            dst[j] = v;
         }
-        for (uint32_t d = threadIdx.x; d < nb; d += blockDim.x) {
-            const uint32_t b = d ? cnt[d - 1] : 0u, e = cnt[d];
-            for (uint32_t i = b + 1; i < e; i++) {
-                const uint64_t v = dst[i];
-                const uint32_t k = tkey(v);
-                uint32_t j = i;
-                while (j > b && tkey(dst[j - 1]) > k) {
-                    dst[j] = dst[j - 1];
-                    j--;
-                }
-                dst[j] = v;
+    }
+    __syncthreads();
+}
+
+
+constexpr uint32_t kDualBucketBits = 11;
+
+// Insertion sort of dst[b..e) by whole word (one thread).
+__device__ __forceinline__ void insertion_words(uint64_t *dst, uint32_t b, uint32_t e) {
+    for (uint32_t i = b + 1; i < e; i++) {
+        const uint64_t v = dst[i];
+        uint32_t j = i;
+        while (j > b && dst[j - 1] > v) {
+            dst[j] = dst[j - 1];
+            j--;
+        }
+        dst[j] = v;
+    }
+}
+
+// Bucket function and outcome of dual_chunk_sort.
+struct DualSort {
+    uint32_t shift, bmask, nb;   // bucket(v) = v == ~0 ? nb : (key >> shift) & bmask
+    bool bitonic;                // a side took the bitonic path: bucket ends are not valid
+    bool max_key;                // a word other than all-ones has key 0xFFFFFFFF
+    __device__ __forceinline__ uint32_t bucket(uint64_t v) const {
+        return v == ~0ULL ? nb : (tkey(v) >> shift) & bmask;
+    }
+};
+
+// chunk_sort of two chunks at once with one bucket function: X[0..nx) -> Xo
+// and Y[0..ny) -> Yo, in the same order rules, with about half the barriers
+// of two calls.  Yo may be X's buffer (X is consumed first); Xo, X and Y must
+// be distinct.  cnt holds 2 * (2^11 + 2) counters: afterwards cnt[d] /
+// cnt[nb + 1 + d] is the end of bucket d of Xo / Yo (unless bitonic).  red
+// holds 96 scratch words.
+__device__ __forceinline__ DualSort dual_chunk_sort(const uint64_t *X, uint32_t nx, uint64_t *Xo, const uint64_t *Y,
+                                                    uint32_t ny, uint64_t *Yo, uint32_t *cnt, uint32_t *red) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nw = (int)(blockDim.x >> 5);
+    uint32_t a = 0xFFFFFFFFu, o = 0, mk = 0;
+    for (uint32_t i = threadIdx.x; i < nx + ny; i += blockDim.x) {
+        const uint64_t v = i < nx ? X[i] : Y[i - nx];
+        if (v != ~0ULL) {
+            a &= tkey(v);
+            o |= tkey(v);
+            mk |= tkey(v) == 0xFFFFFFFFu;
+        }
+    }
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) {
+        a &= __shfl_xor_sync(0xffffffffu, a, s);
+        o |= __shfl_xor_sync(0xffffffffu, o, s);
+        mk |= __shfl_xor_sync(0xffffffffu, mk, s);
+    }
+    if (lane == 0) { red[wid] = a; red[32 + wid] = o; red[64 + wid] = mk; }
+    __syncthreads();
+    a = lane < nw ? red[lane] : 0xFFFFFFFFu;
+    o = lane < nw ? red[32 + lane] : 0u;
+    mk = lane < nw ? red[64 + lane] : 0u;
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) {
+        a &= __shfl_xor_sync(0xffffffffu, a, s);
+        o |= __shfl_xor_sync(0xffffffffu, o, s);
+        mk |= __shfl_xor_sync(0xffffffffu, mk, s);
+    }
+    DualSort r;
+    const uint32_t vary = (a & ~o) ? 0u : a ^ o;
+    const uint32_t hi = vary ? 31 - __clz(vary) : 0u;
+    const uint32_t nbits = vary == 0 ? 0u : (hi + 1 < kDualBucketBits ? hi + 1 : kDualBucketBits);
+    r.shift = vary == 0 ? 0u : hi + 1 - nbits;
+    r.nb = 1u << nbits;
+    r.bmask = r.nb - 1;
+    r.max_key = mk != 0;
+    const uint32_t nb = r.nb, W = nb + 1;   // counters per side; [nb] = all-ones words
+    uint32_t *cx = cnt, *cy = cnt + W;
+    for (uint32_t d = threadIdx.x; d < 2 * W; d += blockDim.x) cnt[d] = 0;
+    __syncthreads();   // also: every thread has read red
+    for (uint32_t i = threadIdx.x; i < nx + ny; i += blockDim.x) {
+        if (i < nx) atomicAdd(&cx[r.bucket(X[i])], 1u);
+        else atomicAdd(&cy[r.bucket(Y[i - nx])], 1u);
+    }
+    __syncthreads();
+    {   // one exclusive scan over cx then cy; cy's offsets restart at 0 (cx totals nx)
+        const uint32_t per = (2 * W + blockDim.x - 1) / blockDim.x;
+        const uint32_t d0 = threadIdx.x * per, d1 = min(2 * W, d0 + per);
+        uint32_t loc = 0;
+        for (uint32_t d = d0; d < d1; d++) loc += cnt[d];
+        uint32_t tot;
+        uint32_t ex = block_exclusive_scan(loc, red, &tot);
+        for (uint32_t d = d0; d < d1; d++) {
+            const uint32_t c = cnt[d];
+            cnt[d] = d < W ? ex : ex - nx;
+            ex += c;
+        }
+    }
+    __syncthreads();
+    // X first: Yo may be X's own buffer
+    for (uint32_t i = threadIdx.x; i < nx; i += blockDim.x) {
+        const uint64_t v = X[i];
+        Xo[atomicAdd(&cx[r.bucket(v)], 1u)] = v;
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < ny; i += blockDim.x) {
+        const uint64_t v = Y[i];
+        Yo[atomicAdd(&cy[r.bucket(v)], 1u)] = v;
+    }
+    __syncthreads();
+    // cx / cy[d] = end of bucket d; which buckets need whole-word order: see chunk_sort
+    const uint32_t d_first = r.shift == 0 ? ((a | r.bmask) == 0xFFFFFFFFu ? r.bmask : nb) : 0u;
+    int big = 0;
+    for (uint32_t d = d_first + threadIdx.x; d < nb; d += blockDim.x) {
+        if (cx[d] - (d ? cx[d - 1] : 0u) > 128) big |= 1;
+        if (cy[d] - (d ? cy[d - 1] : 0u) > 128) big |= 2;
+    }
+    const int bigx = __syncthreads_or(big & 1), bigy = __syncthreads_or(big & 2);
+    if (!bigx || !bigy) {
+        const uint32_t sides = (bigx ? 0u : 1u) | (bigy ? 0u : 2u);
+        for (uint32_t t = d_first + threadIdx.x; t < 2 * nb; t += blockDim.x) {
+            if (t < nb) {
+                if (sides & 1) insertion_words(Xo, t ? cx[t - 1] : 0u, cx[t]);
+            } else if (t - nb >= d_first && (sides & 2)) {
+                const uint32_t d = t - nb;
+                insertion_words(Yo, d ? cy[d - 1] : 0u, cy[d]);
             }
         }
         __syncthreads();
     }
+    if (bigx) bitonic_words(Xo, nx);
+    if (bigy) bitonic_words(Yo, ny);
+    r.bitonic = bigx || bigy;
+    return r;
 }
 
 
