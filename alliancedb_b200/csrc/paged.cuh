@@ -127,10 +127,10 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x, int lane) {
 // unit of a segment).  Per tile of up to kPTile tuples:
 //   A  every thread ranks its tuples within their digit (shared atomics on
 //      cnt[tile parity][d]);
-//   B  warp 0 alone turns the counts into the tile's digit runs (toff), takes
-//      the pages each digit's stream needs from the CTA's pool, and advances
-//      the streams (npos = next free slot of the digit's current page, kNone
-//      when there is none);
+//   B  warps 0 .. F/32 - 1 (one digit per lane) turn the counts into the
+//      tile's digit runs (toff), take the pages each digit's stream needs from
+//      the CTA's pool, and advance the streams (npos = next free slot of the
+//      digit's current page, kNone when there is none);
 //   C  every thread puts its tuples into the stage, grouped by digit;
 //   D  every thread copies stage slots to their pages: slot i of digit d goes
 //      to i + b1[d] while i < lim[d] (the rest of the current page), else to
@@ -138,8 +138,8 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x, int lane) {
 // Consecutive stage slots of a digit go to consecutive addresses, so warps
 // store contiguous runs; a run's partial first and last 32-byte sectors are
 // completed by the neighbouring tiles of the same stream while the line is
-// still in L2.  Three barriers per tile; the next tile's loads are in flight
-// during D.  kMode: 0 flat input, 1 paged input (pass 2), 2 segmented flat
+// still in L2.  Three barriers per tile (four above 32 digits); the next
+// tile's loads are in flight during D.  kMode: 0 flat input, 1 paged input (pass 2), 2 segmented flat
 // input (batched windows).
 template <int kMode, int kThreads>
 __global__ void __launch_bounds__(kThreads, kPassMinBlocks)
@@ -147,6 +147,7 @@ partition_pass(PassArgs a) {
     constexpr bool kPaged = kMode == 1;
     constexpr int kPer = kPTile / kThreads;
     static_assert(kPer % 2 == 0 && kThreads % 32 == 0 && (kPTile / kPageTuples) % (kThreads / 32) == 0, "tile shape");
+    static_assert((1u << kMaxPassBits) <= (uint32_t)kThreads, "one digit per thread in step B");
     extern __shared__ __align__(16) unsigned char smem[];
     const int relidx = blockIdx.y, g = blockIdx.x;
     const PassIn &in = relidx ? a.in[1] : a.in[0];
@@ -183,7 +184,8 @@ partition_pass(PassArgs a) {
     uint32_t *b1 = lim + F;
     uint32_t *b2 = b1 + F;
     uint32_t *npos = b2 + F;
-    uint32_t *misc = npos + F;          // [0] pool pages taken, [1] tuples in the tile
+    uint32_t *misc = npos + F;          // [0] pool pages taken, [1] tuples in the tile,
+                                        // [8..24) per-warp totals of the digit scan
     uint32_t *upage = misc + 48;        // paged input: this unit's pages
     uint8_t *ucnt = reinterpret_cast<uint8_t *>(upage + kMaxUnitPages);
 
@@ -271,31 +273,46 @@ partition_pass(PassArgs a) {
             if (k & 1) rk[k / 2] |= r << 16; else rk[k / 2] = r;
         }
         __syncthreads();
-        // B. warp 0: digit runs of the tile, pages, stream positions
-        if (tid < 32) {
-            uint32_t run = 0, pages = 0;   // running totals over the digits done
-            const uint32_t pool0 = misc[0];
-            for (uint32_t d0 = 0; d0 < F; d0 += 32) {
-                const uint32_t d = d0 + lane;
-                uint32_t L = 0, p = kNone, room = 0, need = 0;
+        // B. digit runs of the tile, pages, stream positions: warp w < F / 32
+        //    handles digits 32w .. 32w + 31, one per lane; the warps' totals are
+        //    combined through shared memory (one extra barrier when F > 32)
+        {
+            const uint32_t nbw = (F + 31) / 32;                 // B warps
+            const int bw = tid >> 5;
+            const uint32_t d = (uint32_t)tid;                   // this lane's digit
+            uint32_t L = 0, p = kNone, room = 0, need = 0, inc = 0, pool0 = 0;
+            if (bw < (int)nbw) {
                 if (d < F) {
                     L = c[d];
                     p = npos[d];
                     room = p == kNone ? 0u : kPageTuples - (p & (kPageTuples - 1));
                     need = L > room ? (L - room + kPageTuples - 1) / kPageTuples : 0u;
                 }
-                const uint32_t v = L | (need << 16);   // L <= kPTile, pages per 32 digits < 2^16
-                const uint32_t inc = warp_incl_scan(v, lane);
-                const uint32_t ex = inc - v;
+                inc = warp_incl_scan(L | (need << 16), lane);   // L <= kPTile, pages of 32 digits < 2^16
+                pool0 = misc[0];
+                if (nbw > 1 && lane == 31) misc[8 + bw] = inc;
+            }
+            if (nbw > 1) __syncthreads();   // every B warp has read misc[0] and written its total
+            if (bw < (int)nbw) {
+                // totals of the warps before this one, and of all of them
+                const uint32_t own = __shfl_sync(0xffffffffu, inc, 31);
+                uint32_t before_t = 0, before_p = 0, all_t = 0, all_p = 0;
+                for (uint32_t k = 0; k < nbw; k++) {
+                    const uint32_t tv = nbw > 1 ? misc[8 + k] : own;
+                    if ((int)k < bw) { before_t += tv & 0xFFFFu; before_p += tv >> 16; }
+                    all_t += tv & 0xFFFFu;
+                    all_p += tv >> 16;
+                }
+                const uint32_t ex = inc - (L | (need << 16));
                 if (d < F) {
-                    const uint32_t off = run + (ex & 0xFFFFu);
+                    const uint32_t off = before_t + (ex & 0xFFFFu);
                     c[d] = 0;
                     toff[d] = off;
                     lim[d] = off + (L < room ? L : room);
                     b1[d] = p - off;
                     uint32_t np = p + L;
                     if (need) {
-                        uint32_t first = pool0 + pages + (ex >> 16);
+                        uint32_t first = pool0 + before_p + (ex >> 16);
                         if (first + need > pool_cap) {   // cannot happen: the pool covers the input
                             atomicExch(a.err, 3);
                             first = pool_cap - need;
@@ -311,13 +328,10 @@ partition_pass(PassArgs a) {
                     if (L && (np & (kPageTuples - 1)) == 0) np = kNone;   // page exactly full
                     npos[d] = np;
                 }
-                const uint32_t tot = __shfl_sync(0xffffffffu, inc, 31);
-                run += tot & 0xFFFFu;
-                pages += tot >> 16;
-            }
-            if (lane == 0) {
-                misc[0] = pool0 + pages;
-                misc[1] = run;
+                if (bw == 0 && lane == 0) {   // warp 0 read misc[0] before the shuffle above
+                    misc[0] = pool0 + all_p;
+                    misc[1] = all_t;
+                }
             }
         }
         __syncthreads();
