@@ -261,7 +261,25 @@ partition_pass(PassArgs a) {
         }
     };
 
-    if (b < e) load_tile(b);
+    // L2 prefetch of a whole tile (flat: one bulk prefetch; paged: one per page)
+    auto prefetch_tile = [&](uint64_t t0) {
+        if (t0 >= e) return;
+        if (kPaged) {
+            const uint64_t li = t0 + tid;
+            if (tid < (int)kStep && li < e) {
+                const uint32_t c = ucnt[li - b];
+                if (c) prefetch_l2(in.pages + (uint64_t)upage[li - b] * kPageTuples, ((c + 1) & ~1u) * 8);
+            }
+        } else if (vec && tid == 0) {
+            const uint64_t n = min(kStep, e - t0) & ~1ull;   // 16-byte multiple
+            if (n) prefetch_l2(in.in + t0, (uint32_t)(n * 8));
+        }
+    };
+
+    if (b < e) {
+        prefetch_tile(b + kStep);
+        load_tile(b);
+    }
     uint32_t par = 0;
     for (uint64_t t0 = b; t0 < e; t0 += kStep, par ^= F) {
         uint32_t *c = cnt + par;
@@ -341,7 +359,10 @@ partition_pass(PassArgs a) {
             if ((valid >> k) & 1)
                 stage[toff[df(tkey(w[k]))] + ((rk[k / 2] >> ((k & 1) * 16)) & 0xFFFFu)] = w[k];
         const uint32_t tile_n = misc[1];
-        if (t0 + kStep < e) load_tile(t0 + kStep);   // in flight during D
+        if (t0 + kStep < e) {   // in flight during D; the tile after that into L2
+            prefetch_tile(t0 + 2 * kStep);
+            load_tile(t0 + kStep);
+        }
         __syncthreads();
         // D. stage slots to their pages
         for (uint32_t i = tid; i < tile_n; i += kThreads) {

@@ -14,6 +14,11 @@ __device__ __forceinline__ uint64_t ld_stream(const uint64_t *p) {
     return __ldcs(reinterpret_cast<const unsigned long long *>(p));
 }
 
+// Bulk prefetch of [p, p + bytes) into L2 (p 16-byte aligned, bytes a multiple of 16).
+__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 struct DigitFn {
     uint32_t kmin;
     uint32_t shift;

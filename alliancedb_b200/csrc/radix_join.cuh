@@ -166,6 +166,32 @@ __device__ __forceinline__ void take_item(uint32_t *work_counter, const uint32_t
     }
 }
 
+// Page ranges of one work item (R chunk pages [rb, rb + nrpg) and S pages
+// [sb, sb + nspg) of its partition's page lists), kept in shared memory so the
+// whole CTA reads them once warp 0 has taken the item.
+struct ItemGeo {
+    uint64_t rb, sb;
+    uint32_t nrpg, nspg;
+};
+
+template <typename Args>
+__device__ __forceinline__ ItemGeo item_geo(const Args &a, uint32_t item, uint32_t p, uint32_t s_pages) {
+    const uint64_t *pR = a.pstart, *pS = a.pstart + (a.F + 1);
+    const uint64_t r0 = pR[p], nrp = pR[p + 1] - r0;
+    const uint64_t s0 = pS[p], nsp = pS[p + 1] - s0;
+    const uint32_t sch = (uint32_t)((nsp + s_pages - 1) / s_pages);
+    const uint32_t local = item - a.items_off[p];
+    const uint32_t rc = local / sch, sc = local % sch;
+    const uint32_t cid = a.chunk_off[p] + rc;
+    ItemGeo g;
+    g.rb = a.cstart[cid];
+    const uint64_t re = rc + 1 < a.chunk_off[p + 1] - a.chunk_off[p] ? a.cstart[cid + 1] : r0 + nrp;
+    g.nrpg = (uint32_t)(re - g.rb);
+    g.sb = s0 + (uint64_t)sc * s_pages;
+    g.nspg = (uint32_t)min((uint64_t)s_pages, nsp - (uint64_t)sc * s_pages);
+    return g;
+}
+
 // --- bulk async copy helpers (sm_90+ PTX) -----------------------------------
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
     const uint32_t a = (uint32_t)__cvta_generic_to_shared(bar);
@@ -253,37 +279,34 @@ radix_join_items(JoinArgs a) {
     uint32_t *pcnt = pdst + kRMaxPages + 1;
     uint64_t *bar = reinterpret_cast<uint64_t *>(pcnt + kRMaxPages + 1);
     uint64_t *red = bar + 2;
-    uint32_t *slots = reinterpret_cast<uint32_t *>(red + 64);            // [0] item, [4..36) scan scratch
+    uint32_t *slots = reinterpret_cast<uint32_t *>(red + 64);            // [0..3) item, [4..36) scan scratch
+    ItemGeo *geo = reinterpret_cast<ItemGeo *>(slots + 40);              // page ranges of slots[0]
 
     const uint32_t n_items = *a.n_items;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int kWarps = kJoinThreads / 32;
+    // warp 0: take the next item and publish its page ranges
+    auto next_item = [&]() {
+        take_item(a.work_counter, a.items_off, a.F, n_items, a.wacc ? a.wbase : nullptr, a.nwin, slots, lane);
+        __syncwarp();
+        if (lane == 0 && slots[0] < n_items) *geo = item_geo(a, slots[0], slots[1], kSPages);
+    };
     if (threadIdx.x == 0) mbar_init(bar, 1);
-    if (warp == 0) take_item(a.work_counter, a.items_off, a.F, n_items, a.wacc ? a.wbase : nullptr, a.nwin, slots, lane);
+    if (warp == 0) next_item();
     __syncthreads();
     uint32_t phase = 0;
     Acc acc;
     const uint32_t F = a.F;
-    const uint64_t *pR = a.pstart, *pS = a.pstart + (F + 1);
 
     while (true) {
-        // the item taken during the previous item's probe (or before the loop)
+        // the item taken during the previous item's build (or before the loop)
         const uint32_t item = slots[0];
         if (item >= n_items) break;
-        const uint32_t p = slots[1];
         const uint32_t win = slots[2];
         const uint32_t shift = a.wacc ? a.wbits[win] : a.bits;
-        const uint64_t r0 = pR[p], nrp = pR[p + 1] - r0;
-        const uint64_t s0 = pS[p], nsp = pS[p + 1] - s0;
-        const uint32_t sch = (uint32_t)((nsp + kSPages - 1) / kSPages);
-        const uint32_t local = item - a.items_off[p];
-        const uint32_t rc = local / sch, sc = local % sch;
-        const uint32_t cid = a.chunk_off[p] + rc;
-        const uint64_t rb = a.cstart[cid];
-        const uint64_t re = rc + 1 < a.chunk_off[p + 1] - a.chunk_off[p] ? a.cstart[cid + 1] : r0 + nrp;
-        const uint32_t nrpg = (uint32_t)(re - rb);
-        const uint64_t sb = s0 + (uint64_t)sc * kSPages;
-        const uint32_t nspg = (uint32_t)min((uint64_t)kSPages, nsp - (uint64_t)sc * kSPages);
+        const ItemGeo cur = *geo;
+        const uint64_t rb = cur.rb, sb = cur.sb;
+        const uint32_t nrpg = cur.nrpg, nspg = cur.nspg;
 
         // --- S chunk metadata and each warp's first page: issued now, used after the build.
         //     Warp w takes pages w, w + kWarps, ...: lane i holds the id and count of
@@ -335,6 +358,9 @@ radix_join_items(JoinArgs a) {
                          bar);
             }
         }
+        // every thread has read this item's slots and ranges (barrier above):
+        // warp 0 takes the next item, visible to all after the barrier below
+        if (warp == 0) next_item();
 
         uint32_t nb = 1;
         while (nb < tot_slots) nb <<= 1;
@@ -401,8 +427,21 @@ radix_join_items(JoinArgs a) {
         }
 
         // --- probe the S chunk; the next page of a warp is loaded before the
-        //     current one is probed, and warp 0 first takes the next item
-        if (warp == 0) take_item(a.work_counter, a.items_off, F, n_items, a.wacc ? a.wbase : nullptr, a.nwin, slots, lane);
+        //     current one is probed.  Thread t also prefetches page t of the
+        //     next item's R chunk and S chunk into L2 (whole pages; R chunks
+        //     have < kJoinThreads pages, S chunks at most kSPages), so that
+        //     item's bulk copies and S loads find their data in L2.
+        uint32_t nx_r = kNone, nx_s = kNone;
+        if (slots[0] < n_items) {
+            const ItemGeo nx = *geo;
+            if (threadIdx.x < nx.nrpg) nx_r = a.Rlist[nx.rb + threadIdx.x];
+            if (threadIdx.x < nx.nspg) nx_s = a.Slist[nx.sb + threadIdx.x];
+        }
+        auto prefetch_next = [&]() {
+            if (nx_r != kNone) prefetch_l2(a.Rpages + (uint64_t)nx_r * kPageTuples, kPageTuples * 8);
+            if (nx_s != kNone) prefetch_l2(a.Spages + (uint64_t)nx_s * kPageTuples, kPageTuples * 8);
+        };
+        if (npw == 0) prefetch_next();
         {
             for (uint32_t i = 0; i < npw; i++) {
                 uint64_t n0 = 0, n1 = 0;
@@ -446,6 +485,7 @@ radix_join_items(JoinArgs a) {
                     }
                 }
                 c0 = n0; c1 = n1; ccnt = ncnt;
+                if (i == 0) prefetch_next();   // the page ids have arrived meanwhile
             }
         }
         if (a.wacc) {   // batched windows: this item's sums to its window

@@ -243,6 +243,8 @@ def main():
                          "stream: two timestamped streams in 1000 ms tumbling windows")
     ap.add_argument("--windows", type=int, default=4096)
     ap.add_argument("--requests", type=int, default=4000)
+    ap.add_argument("--radix-bits", type=int, default=0,
+                    help="partitioned joins: fan-out bits (0 = the library's choice)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -279,8 +281,10 @@ def main():
     stream = torch.cuda.current_stream(dev)
     sp = stream.cuda_stream
 
+    params = adb.default_params(radix_bits=args.radix_bits) if args.radix_bits else None
+
     def step():
-        return adb.join_device(args.algo, dR.data_ptr(), n, dS.data_ptr(), n, None, sp)
+        return adb.join_device(args.algo, dR.data_ptr(), n, dS.data_ptr(), n, params, sp)
 
     def barrier():
         if dist is not None:
@@ -314,7 +318,8 @@ def main():
     res = adb.JoinResult()
 
     def step_e2e():
-        st = L.adb_join(args.algo.encode(), hR.data_ptr(), n, hS.data_ptr(), n, None, C.byref(res))
+        st = L.adb_join(args.algo.encode(), hR.data_ptr(), n, hS.data_ptr(), n,
+                        C.byref(params) if params is not None else None, C.byref(res))
         if st != 0:
             raise RuntimeError(L.adb_last_error().decode())
         return res

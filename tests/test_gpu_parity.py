@@ -79,9 +79,17 @@ def test_empty(oracle, algo):
 
 
 @pytest.mark.parametrize("algo", ["PRO", "PRH", "NPO"])
-@pytest.mark.parametrize("bits", [1, 4, 8, 13])
+@pytest.mark.parametrize("bits", [1, 4, 8, 9, 10, 11, 12, 13, 14])
 def test_radix_bits(oracle, algo, bits):
     R, S = fk_pair(50000, 70001, 0.8)
+    check(oracle, algo, R, S, radix_bits=bits)
+
+
+@pytest.mark.parametrize("algo", ["PRO", "PRH"])
+@pytest.mark.parametrize("bits", [10, 13])
+def test_wide_pass_sizes(oracle, algo, bits):
+    """One-pass fan-outs of 2^10 .. 2^13 over several tiles per CTA, skewed S."""
+    R, S = fk_pair((1 << 21) + 5, (1 << 21) + 77, 1.0)
     check(oracle, algo, R, S, radix_bits=bits)
 
 
