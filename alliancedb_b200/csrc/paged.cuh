@@ -261,16 +261,12 @@ partition_pass(PassArgs a) {
         }
     };
 
-    // L2 prefetch of a whole tile (flat: one bulk prefetch; paged: one per page)
+    // L2 prefetch of a whole flat tile (one bulk prefetch; paged input is not
+    // prefetched: one bulk prefetch per 512-byte page costs the SM's bulk-copy
+    // unit more than the latency it hides)
     auto prefetch_tile = [&](uint64_t t0) {
         if (t0 >= e) return;
-        if (kPaged) {
-            const uint64_t li = t0 + tid;
-            if (tid < (int)kStep && li < e) {
-                const uint32_t c = ucnt[li - b];
-                if (c) prefetch_l2(in.pages + (uint64_t)upage[li - b] * kPageTuples, ((c + 1) & ~1u) * 8);
-            }
-        } else if (vec && tid == 0) {
+        if (!kPaged && vec && tid == 0) {
             const uint64_t n = min(kStep, e - t0) & ~1ull;   // 16-byte multiple
             if (n) prefetch_l2(in.in + t0, (uint32_t)(n * 8));
         }

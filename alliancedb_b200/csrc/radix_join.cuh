@@ -26,7 +26,8 @@ constexpr uint32_t kRSlots = 17408;                        // R tuples a CTA hol
 constexpr uint32_t kChunkW = kRSlots - kPageTuples;        // chunk weight budget
 constexpr uint32_t kMinPageW = 32;                         // weight floor of a page
 constexpr uint32_t kRMaxPages = kChunkW / kMinPageW + 16;  // pages of one R chunk (bound)
-constexpr uint32_t kSPages = kJoinThreads;                 // S pages per item: <= 32 per warp (one per lane)
+constexpr int kProbeWarps = kJoinThreads / 32 - 1;        // the last warp is the control warp
+constexpr uint32_t kSPages = kProbeWarps * 32;             // S pages per item: <= 32 per probing warp (one per lane)
 constexpr uint32_t kMaxHeads = kRSlots >= 16384 ? 8192 : 4096;   // Chain: bucket heads (~2 slots each)
 constexpr uint32_t kMaxHist = kMaxHeads / 4;               // Hist: buckets
 
@@ -226,19 +227,19 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t phase) {
 
 enum class TableKind { Chain = 0, Hist = 1 };
 
-// Shared memory: tup[kRSlots] u64 | aux[kRSlots] u16 | X | pdst[kRMaxPages + 1],
-// pcnt[kRMaxPages + 1] u32 | mbarrier, reduction, item slot and scan scratch.
+// Shared memory: tup[kRSlots] u64 | aux[kRSlots] u16 | X | two page tables
+// {pg[kRMaxPages + 1] u32, dst << 8 | count [kRMaxPages + 1] u32} | mbarrier,
+// reduction, two item records and scan scratch.
 // X holds the Chain heads (kMaxHeads u32) or the Hist permutation (kRSlots u16)
 // followed by its bucket starts (kMaxHist + 2 u32).
 constexpr size_t kXBytes = ((size_t)kRSlots * 2 + ((size_t)kMaxHist + 2) * 4) > (size_t)kMaxHeads * 4
                                ? ((size_t)kRSlots * 2 + ((size_t)kMaxHist + 2) * 4 + 15) & ~(size_t)15
                                : (size_t)kMaxHeads * 4;
-constexpr size_t kJoinSmem = (size_t)kRSlots * 8 + (size_t)kRSlots * 2 + kXBytes +
-                             ((size_t)kRMaxPages + 1) * 4 * 2 + 1024;
-static_assert(((size_t)kRSlots * 10 + kXBytes + ((size_t)kRMaxPages + 1) * 8) % 8 == 0,
-              "mbarrier must be 8-byte aligned");
+constexpr size_t kPageTabBytes = ((size_t)kRMaxPages + 1) * 4 * 2;
+constexpr size_t kJoinSmem = (size_t)kRSlots * 8 + (size_t)kRSlots * 2 + kXBytes + 2 * kPageTabBytes + 1024;
+static_assert(((size_t)kRSlots * 10 + kXBytes + 2 * kPageTabBytes) % 8 == 0, "mbarrier must be 8-byte aligned");
 static_assert(kJoinMinBlocks * (kJoinSmem + 1024) <= 233472, "join CTAs exceed the SM's shared memory");
-static_assert(kSPages <= 32 * (kJoinThreads / 32), "a warp's S pages are held one per lane");
+static_assert(kRSlots < (1u << 24) && kRMaxPages < (uint32_t)kJoinThreads, "page table packing");
 
 struct JoinArgs {
     const uint64_t *Rpages, *Spages;
@@ -265,6 +266,24 @@ struct JoinArgs {
     unsigned long long *wacc;
 };
 
+// One work item as the control warp publishes it.
+struct ItemRec {
+    uint64_t rb, sb;          // first page-list index of the R chunk / S chunk
+    uint32_t item, p, win;    // item (>= n_items: none), partition, window
+    uint32_t nrpg, nspg;      // pages of the R chunk / S chunk
+    uint32_t rslots;          // R chunk slots in shared memory (pages rounded up to even counts)
+};
+
+// The items of one CTA form a pipeline run by its last warp (the control
+// warp), so that no dependent global load sits between two items:
+//   while item i is probed, the control warp builds the page table of item
+//   i + 1 (page ids, 16-byte aligned shared-memory destinations) and takes
+//   item i + 2 from the work counter; the probing warps load their S page ids
+//   of item i + 1.
+// Per item: one bulk async copy per R page (cp.async.bulk global -> shared,
+// completion counted on an mbarrier with a bounded wait), the table build by
+// all warps, then the probe by warps 0 .. kProbeWarps - 1, each holding two S
+// pages in flight ahead of the one it probes.
 template <TableKind K>
 __global__ void __launch_bounds__(kJoinThreads, kJoinMinBlocks)
 radix_join_items(JoinArgs a) {
@@ -275,95 +294,149 @@ radix_join_items(JoinArgs a) {
     uint16_t *perm = reinterpret_cast<uint16_t *>(xr);                   // Hist: bucket-ordered slots
     uint32_t *heads = K == TableKind::Chain ? reinterpret_cast<uint32_t *>(xr)      // Chain: heads
                                             : reinterpret_cast<uint32_t *>(perm + kRSlots);  // Hist: starts
-    uint32_t *pdst = reinterpret_cast<uint32_t *>(xr + kXBytes);
-    uint32_t *pcnt = pdst + kRMaxPages + 1;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(pcnt + kRMaxPages + 1);
+    uint32_t *ptab = reinterpret_cast<uint32_t *>(xr + kXBytes);         // [2] x {pg[], dst << 8 | cnt []}
+    uint64_t *bar = reinterpret_cast<uint64_t *>(ptab + 4 * (kRMaxPages + 1));
     uint64_t *red = bar + 2;
-    uint32_t *slots = reinterpret_cast<uint32_t *>(red + 64);            // [0..3) item, [4..36) scan scratch
-    ItemGeo *geo = reinterpret_cast<ItemGeo *>(slots + 40);              // page ranges of slots[0]
+    ItemRec *rec = reinterpret_cast<ItemRec *>(red + 64);                // [2]
+    uint32_t *scan = reinterpret_cast<uint32_t *>(rec + 2);              // 32 u32
 
     const uint32_t n_items = *a.n_items;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int kWarps = kJoinThreads / 32;
-    // warp 0: take the next item and publish its page ranges
-    auto next_item = [&]() {
-        take_item(a.work_counter, a.items_off, a.F, n_items, a.wacc ? a.wbase : nullptr, a.nwin, slots, lane);
-        __syncwarp();
-        if (lane == 0 && slots[0] < n_items) *geo = item_geo(a, slots[0], slots[1], kSPages);
-    };
-    if (threadIdx.x == 0) mbar_init(bar, 1);
-    if (warp == 0) next_item();
-    __syncthreads();
-    uint32_t phase = 0;
-    Acc acc;
+    constexpr int kCtl = kWarps - 1;
     const uint32_t F = a.F;
 
-    while (true) {
-        // the item taken during the previous item's build (or before the loop)
-        const uint32_t item = slots[0];
-        if (item >= n_items) break;
-        const uint32_t win = slots[2];
-        const uint32_t shift = a.wacc ? a.wbits[win] : a.bits;
-        const ItemGeo cur = *geo;
-        const uint64_t rb = cur.rb, sb = cur.sb;
-        const uint32_t nrpg = cur.nrpg, nspg = cur.nspg;
-
-        // --- S chunk metadata and each warp's first page: issued now, used after the build.
-        //     Warp w takes pages w, w + kWarps, ...: lane i holds the id and count of
-        //     the warp's i-th page.
-        const uint32_t npw = warp < (int)nspg ? (nspg - warp + kWarps - 1) / kWarps : 0;
-        uint32_t my_pg = 0, my_cnt = 0;
-        if (lane < (int)npw) {
-            my_pg = a.Slist[sb + warp + (uint64_t)kWarps * lane];
-            my_cnt = a.Scount[my_pg];
+    // control warp: take the next item from the work counter into r
+    auto take = [&](ItemRec *r) {
+        uint32_t item = 0;
+        if (lane == 0) item = atomicAdd(a.work_counter, 1u);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        uint32_t p = 0, w = 0;
+        if (item < n_items) {
+            p = warp_find(a.items_off, F, item, lane);
+            if (a.wacc) w = warp_find(a.wbase, a.nwin, p, lane);
         }
+        if (lane == 0) {
+            r->item = item;
+            if (item < n_items) {
+                const ItemGeo g = item_geo(a, item, p, kSPages);
+                r->p = p;
+                r->win = w;
+                r->rb = g.rb;
+                r->sb = g.sb;
+                r->nrpg = g.nrpg;
+                r->nspg = g.nspg;
+            }
+        }
+        __syncwarp();
+    };
+    // control warp: page table of item r (page ids, packed destination and
+    // count) and the mbarrier's expected bytes for its copies.  (No bulk L2
+    // prefetch of the pages: one cp.async.bulk.prefetch per 512-byte page
+    // occupies the SM's bulk-copy unit for tens of cycles and delays the
+    // item's own copies.)
+    auto table = [&](ItemRec *r, uint32_t *pt) {
+        if (r->item >= n_items) return;
+        const uint64_t rb = r->rb;
+        const uint32_t nrpg = r->nrpg;
+        uint32_t *tpg = pt, *tpk = pt + kRMaxPages + 1;
+        uint32_t carry = 0;
+        constexpr int U = 4;
+        for (uint32_t base = 0; base < nrpg; base += 32 * U) {
+            uint32_t pg[U], cnt[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const uint32_t k = base + 32 * u + lane;
+                pg[u] = k < nrpg ? a.Rlist[rb + k] : kNone;
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) cnt[u] = pg[u] != kNone ? a.Rcount[pg[u]] : 0u;
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const uint32_t k = base + 32 * u + lane;
+                const uint32_t e = (cnt[u] + 1) & ~1u;
+                const uint32_t inc = warp_incl_scan(e, lane);
+                if (k < nrpg) {
+                    tpg[k] = pg[u];
+                    tpk[k] = ((carry + inc - e) << 8) | cnt[u];
+                }
+                carry += __shfl_sync(0xffffffffu, inc, 31);
+            }
+        }
+        if (lane == 0) {
+            r->rslots = carry;
+            // the item's copies are issued after the next barrier; the barrier
+            // is in the item's phase already (the previous item's copies landed)
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_expect_tx(bar, carry * 8);
+        }
+        __syncwarp();
+    };
+
+    if (threadIdx.x == 0) mbar_init(bar, 1);
+    if (warp == kCtl) {
+        take(&rec[0]);
+        table(&rec[0], ptab);
+        take(&rec[1]);
+    }
+    __syncthreads();
+
+    // S page ids of a probing warp for item r: lane i holds page warp + kProbeWarps * i
+    auto s_ids = [&](const ItemRec &r, uint32_t &pg, uint32_t &cnt) {
+        pg = 0;
+        cnt = 0;
+        if (warp < kProbeWarps && r.item < n_items) {
+            const uint32_t i = (uint32_t)warp + (uint32_t)kProbeWarps * lane;
+            if (i < r.nspg) {
+                pg = a.Slist[r.sb + i];
+                cnt = a.Scount[pg];
+            }
+        }
+    };
+    uint32_t my_pg, my_cnt;
+    s_ids(rec[0], my_pg, my_cnt);
+
+    uint32_t phase = 0;
+    int cur = 0;
+    Acc acc;
+    while (true) {
+        const ItemRec C = rec[cur];
+        if (C.item >= n_items) break;
+        const uint32_t *tpg = ptab + cur * 2 * (kRMaxPages + 1);
+        const uint32_t *tpk = tpg + kRMaxPages + 1;
+        const uint32_t shift = a.wacc ? a.wbits[C.win] : a.bits;
+        const uint32_t nrpg = C.nrpg, nspg = C.nspg;
+
+        // --- R chunk: one bulk copy per page from the page table (the
+        //     control warp announced the bytes when it built the table)
+        for (uint32_t k = threadIdx.x; k < nrpg; k += blockDim.x) {
+            const uint32_t v = tpk[k], cnt = v & 0xFFu;
+            if (cnt) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                bulk_g2s(tup + (v >> 8), a.Rpages + (uint64_t)tpg[k] * kPageTuples, ((cnt + 1) & ~1u) * 8, bar);
+            }
+        }
+
+        // --- the probing warp's first two S pages (ids loaded during the previous item)
+        const uint32_t npw = warp < kProbeWarps && (uint32_t)warp < nspg
+                                 ? (nspg - warp + kProbeWarps - 1) / kProbeWarps : 0u;
         auto load_page = [&](uint32_t i, uint64_t &x0, uint64_t &x1, uint32_t &cn) {
-            const uint32_t pgi = __shfl_sync(0xffffffffu, my_pg, i);
-            cn = __shfl_sync(0xffffffffu, my_cnt, i);
+            const uint32_t pgi = __shfl_sync(0xffffffffu, my_pg, i & 31);
+            cn = __shfl_sync(0xffffffffu, my_cnt, i & 31);
+            if (i >= npw) cn = 0;
             const uint64_t *Sp = a.Spages + (uint64_t)pgi * kPageTuples;
             x0 = lane < (int)cn ? ld_stream(Sp + lane) : 0;
             x1 = lane + 32 < (int)cn ? ld_stream(Sp + lane + 32) : 0;
         };
-        uint64_t c0 = 0, c1 = 0;
-        uint32_t ccnt = 0;
-        if (npw) load_page(0, c0, c1, ccnt);
-
-        // --- R chunk: page counts, 16-byte aligned destinations, one bulk copy per page
-        uint32_t tot_slots = 0;
-        for (uint32_t base = 0; base < nrpg; base += blockDim.x) {
-            const uint32_t k = base + threadIdx.x;
-            uint32_t pg = 0, cnt = 0;
-            if (k < nrpg) {
-                pg = a.Rlist[rb + k];
-                cnt = a.Rcount[pg];
-            }
-            uint32_t tot;
-            const uint32_t dst = tot_slots + block_exclusive_scan((cnt + 1) & ~1u, slots + 4, &tot);
-            if (k < nrpg) {
-                pdst[k] = dst;
-                pcnt[k] = cnt;
-            }
-            tot_slots += tot;
+        uint64_t c0 = 0, c1 = 0, n0 = 0, n1 = 0;
+        uint32_t ccnt = 0, ncnt = 0;
+        if (warp < kProbeWarps) {
+            load_page(0, c0, c1, ccnt);
+            load_page(1, n0, n1, ncnt);
         }
-        if (threadIdx.x == 0) {
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            mbar_expect_tx(bar, tot_slots * 8);
-        }
-        __syncthreads();
-        for (uint32_t k = threadIdx.x; k < nrpg; k += blockDim.x) {
-            const uint32_t cnt = pcnt[k];
-            if (cnt) {
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                bulk_g2s(tup + pdst[k], a.Rpages + (uint64_t)a.Rlist[rb + k] * kPageTuples, ((cnt + 1) & ~1u) * 8,
-                         bar);
-            }
-        }
-        // every thread has read this item's slots and ranges (barrier above):
-        // warp 0 takes the next item, visible to all after the barrier below
-        if (warp == 0) next_item();
 
         uint32_t nb = 1;
-        while (nb < tot_slots) nb <<= 1;
+        while (nb < C.rslots) nb <<= 1;
         if (K == TableKind::Chain) {
             nb >>= 1;                                  // about two slots per head
             if (nb > kMaxHeads) nb = kMaxHeads;
@@ -381,7 +454,7 @@ radix_join_items(JoinArgs a) {
         // --- build (warp per page, two tuples per lane)
         if (K == TableKind::Chain) {
             for (uint32_t k = warp; k < nrpg; k += kWarps) {
-                const uint32_t c = pcnt[k], base = pdst[k];
+                const uint32_t v = tpk[k], c = v & 0xFFu, base = v >> 8;
                 for (uint32_t l = lane; l < c; l += 32) {
                     const uint32_t s = base + l;
                     const uint32_t h = (tkey(tup[s]) >> shift) & bmask;
@@ -391,7 +464,7 @@ radix_join_items(JoinArgs a) {
             __syncthreads();
         } else {
             for (uint32_t k = warp; k < nrpg; k += kWarps) {
-                const uint32_t c = pcnt[k], base = pdst[k];
+                const uint32_t v = tpk[k], c = v & 0xFFu, base = v >> 8;
                 for (uint32_t l = lane; l < c; l += 32) {
                     const uint32_t s = base + l;
                     const uint32_t h = (tkey(tup[s]) >> shift) & bmask;
@@ -405,7 +478,7 @@ radix_join_items(JoinArgs a) {
                 uint32_t loc = 0;
                 for (uint32_t d = d0; d < d1; d++) loc += heads[d + 1];
                 uint32_t tot;
-                uint32_t ex = block_exclusive_scan(loc, slots + 4, &tot);
+                uint32_t ex = block_exclusive_scan(loc, scan, &tot);
                 for (uint32_t d = d0; d < d1; d++) {
                     const uint32_t c = heads[d + 1];
                     heads[d + 1] = ex;
@@ -416,7 +489,7 @@ radix_join_items(JoinArgs a) {
             }
             __syncthreads();
             for (uint32_t k = warp; k < nrpg; k += kWarps) {
-                const uint32_t c = pcnt[k], base = pdst[k];
+                const uint32_t v = tpk[k], c = v & 0xFFu, base = v >> 8;
                 for (uint32_t l = lane; l < c; l += 32) {
                     const uint32_t s = base + l;
                     const uint32_t h = (tkey(tup[s]) >> shift) & bmask;
@@ -426,27 +499,20 @@ radix_join_items(JoinArgs a) {
             __syncthreads();
         }
 
-        // --- probe the S chunk; the next page of a warp is loaded before the
-        //     current one is probed.  Thread t also prefetches page t of the
-        //     next item's R chunk and S chunk into L2 (whole pages; R chunks
-        //     have < kJoinThreads pages, S chunks at most kSPages), so that
-        //     item's bulk copies and S loads find their data in L2.
-        uint32_t nx_r = kNone, nx_s = kNone;
-        if (slots[0] < n_items) {
-            const ItemGeo nx = *geo;
-            if (threadIdx.x < nx.nrpg) nx_r = a.Rlist[nx.rb + threadIdx.x];
-            if (threadIdx.x < nx.nspg) nx_s = a.Slist[nx.sb + threadIdx.x];
-        }
-        auto prefetch_next = [&]() {
-            if (nx_r != kNone) prefetch_l2(a.Rpages + (uint64_t)nx_r * kPageTuples, kPageTuples * 8);
-            if (nx_s != kNone) prefetch_l2(a.Spages + (uint64_t)nx_s * kPageTuples, kPageTuples * 8);
-        };
-        if (npw == 0) prefetch_next();
-        {
+        if (warp == kCtl) {
+            // the next item's page table and prefetches, then the item after it
+            // (rec[cur] is free: every thread copied it before the barriers above)
+            table(&rec[cur ^ 1], ptab + (cur ^ 1) * 2 * (kRMaxPages + 1));
+            take(&rec[cur]);
+        } else {
+            // the next item's S page ids, in flight during this probe
+            uint32_t nx_pg, nx_cnt;
+            s_ids(rec[cur ^ 1], nx_pg, nx_cnt);
+            // --- probe; page i + 2 is loaded before page i is probed
             for (uint32_t i = 0; i < npw; i++) {
-                uint64_t n0 = 0, n1 = 0;
-                uint32_t ncnt = 0;
-                if (i + 1 < npw) load_page(i + 1, n0, n1, ncnt);
+                uint64_t m0 = 0, m1 = 0;
+                uint32_t mcnt = 0;
+                if (i + 2 < npw) load_page(i + 2, m0, m1, mcnt);
 #pragma unroll
                 for (int half = 0; half < 2; half++) {
                     if (lane + 32 * half >= (int)ccnt) continue;
@@ -485,14 +551,17 @@ radix_join_items(JoinArgs a) {
                     }
                 }
                 c0 = n0; c1 = n1; ccnt = ncnt;
-                if (i == 0) prefetch_next();   // the page ids have arrived meanwhile
+                n0 = m0; n1 = m1; ncnt = mcnt;
             }
+            my_pg = nx_pg;
+            my_cnt = nx_cnt;
         }
         if (a.wacc) {   // batched windows: this item's sums to its window
-            block_flush(acc, a.wacc + 2 * win, red);
+            block_flush(acc, a.wacc + 2 * C.win, red);
             acc = Acc();
         }
-        __syncthreads();   // the next item rebuilds the table
+        __syncthreads();   // the next item rebuilds the table; rec / page tables published
+        cur ^= 1;
     }
     block_flush(acc, a.acc, red);
 }
