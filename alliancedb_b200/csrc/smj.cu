@@ -34,11 +34,13 @@ constexpr uint32_t kSmjSPages = kSmjCap / kPageTuples;   // 128 pages <= 8192 tu
 constexpr uint32_t kSmjMaxPages = 272;              // weight floor 32: <= 8192 / 32 + 1 pages per chunk
 constexpr uint32_t kSmjThreads = 1024;
 
-// A | B | C tuple buffers, bucket counters, R and S page tables, barrier and scratch.
-constexpr size_t kSmjSmem = (size_t)kSmjCap * 8 * 3 + ((size_t)(1u << kDualBucketBits) + 2) * 4 * 2 +
-                            ((size_t)kSmjMaxPages + 1) * 4 * 2 + ((size_t)kSmjSPages + 1) * 4 * 2 + 1024;
+// A | B | C tuple buffers, bucket counters, two page tables (R pages then S
+// pages: page id, dst << 8 | count), barrier, scratch and two item records.
+constexpr uint32_t kSmjTabEntries = kSmjMaxPages + kSmjSPages + 1;
+constexpr size_t kSmjSmem = (size_t)kSmjCap * 8 * 3 + (size_t)kDualCntWords * 4 + (size_t)kSmjTabEntries * 4 * 2 * 2 +
+                            1024;
 static_assert(kSmjSmem <= 232448, "smj_items exceeds the 227 KB shared-memory limit");
-static_assert(kSmjMaxPages + kSmjSPages <= kSmjThreads, "one page-table entry per thread");
+static_assert(((size_t)kDualCntWords + (size_t)kSmjTabEntries * 4) % 2 == 0, "mbarrier must be 8-byte aligned");
 
 struct SmjArgs {
     const uint64_t *Rpages, *Spages;
@@ -57,6 +59,18 @@ struct SmjArgs {
     uint64_t mat_cap;
 };
 
+// One work item as the control warp publishes it.
+struct SmjRec {
+    uint64_t rb, sb;                 // first page-list index of the R chunk / S block
+    uint32_t item, nrpg, nspg;       // item (>= n_items: none), pages of each side
+    uint32_t rslots, sslots;         // shared-memory slots of each side (pages rounded up to even)
+    uint32_t rpad, spad;             // odd pages of each side (one all-ones pad word each)
+    uint32_t pad_;
+};
+
+// Items are pipelined as in radix_join_items: while item i is merge-joined by
+// warps 0 .. 30, the last warp builds the page table of item i + 1 and takes
+// item i + 2, so no dependent global load sits between two items.
 __global__ void __launch_bounds__(kSmjThreads, 1)
 smj_items(SmjArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -64,85 +78,127 @@ smj_items(SmjArgs a) {
     uint64_t *B = A + kSmjCap;
     uint64_t *C = B + kSmjCap;
     uint32_t *cnt = reinterpret_cast<uint32_t *>(C + kSmjCap);
-    uint32_t *pdst = cnt + 2 * ((1u << kDualBucketBits) + 2);   // R page table
-    uint32_t *pcnt = pdst + kSmjMaxPages + 1;
-    uint32_t *sdst = pcnt + kSmjMaxPages + 1;                // S page table
-    uint32_t *scnt = sdst + kSmjSPages + 1;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(scnt + kSmjSPages + 1);
+    uint32_t *ptab = cnt + kDualCntWords;                    // [2] x {pg[kSmjTabEntries], dst << 8 | count []}
+    uint64_t *bar = reinterpret_cast<uint64_t *>(ptab + 4 * kSmjTabEntries);
     uint64_t *red = bar + 2;                                 // 64 u64 (96 u32 of sort scratch)
-    uint32_t *slots = reinterpret_cast<uint32_t *>(red + 64);   // [0..3) next item, [4..36) scan scratch
+    SmjRec *rec = reinterpret_cast<SmjRec *>(red + 64);      // [2]
 
     const uint32_t n_items = *a.n_items;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int kWarps = kSmjThreads / 32;
+    constexpr int kCtl = kWarps - 1;
+    constexpr uint32_t kWork = kSmjThreads - 32;             // threads of the merge join
+    const uint32_t F = a.F;
+
+    // control warp: take the next item into r
+    auto take = [&](SmjRec *r) {
+        uint32_t item = 0;
+        if (lane == 0) item = atomicAdd(a.work_counter, 1u);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        uint32_t p = 0;
+        if (item < n_items) p = warp_find(a.items_off, F, item, lane);
+        if (lane == 0) {
+            r->item = item;
+            if (item < n_items) {
+                const ItemGeo g = item_geo(a, item, p, kSmjSPages);
+                r->rb = g.rb;
+                r->sb = g.sb;
+                r->nrpg = g.nrpg;
+                r->nspg = g.nspg;
+            }
+        }
+        __syncwarp();
+    };
+    // control warp: page table of item r (R pages to A, S pages to C, 16-byte
+    // aligned slots), its slot and pad counts, and the mbarrier's expected bytes
+    auto table = [&](SmjRec *r, uint32_t *pt) {
+        if (r->item >= n_items) return;
+        uint32_t *tpg = pt, *tpk = pt + kSmjTabEntries;
+        uint32_t slots_of[2] = {0, 0}, pads_of[2] = {0, 0};
+        constexpr int U = 4;
+#pragma unroll
+        for (int side = 0; side < 2; side++) {
+            const uint32_t n = side ? r->nspg : r->nrpg;
+            const uint64_t b0 = side ? r->sb : r->rb;
+            const uint32_t *list = side ? a.Slist : a.Rlist;
+            const uint8_t *count = side ? a.Scount : a.Rcount;
+            const uint32_t k0 = side ? r->nrpg : 0u;
+            uint32_t carry = 0, pads = 0;
+            for (uint32_t base = 0; base < n; base += 32 * U) {
+                uint32_t pg[U], c[U];
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const uint32_t k = base + 32 * u + lane;
+                    pg[u] = k < n ? list[b0 + k] : kNone;
+                }
+#pragma unroll
+                for (int u = 0; u < U; u++) c[u] = pg[u] != kNone ? count[pg[u]] : 0u;
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const uint32_t k = base + 32 * u + lane;
+                    const uint32_t e = (c[u] + 1) & ~1u;
+                    const uint32_t inc = warp_incl_scan(e, lane);
+                    if (k < n) {
+                        tpg[k0 + k] = pg[u];
+                        tpk[k0 + k] = ((carry + inc - e) << 8) | c[u];
+                    }
+                    carry += __shfl_sync(0xffffffffu, inc, 31);
+                    pads += __popc(__ballot_sync(0xffffffffu, c[u] & 1u));
+                }
+            }
+            slots_of[side] = carry;
+            pads_of[side] = pads;
+        }
+        if (lane == 0) {
+            r->rslots = slots_of[0];
+            r->sslots = slots_of[1];
+            r->rpad = pads_of[0];
+            r->spad = pads_of[1];
+            // the item's copies are issued after the next barrier, in its phase
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_expect_tx(bar, (slots_of[0] + slots_of[1]) * 8);
+        }
+        __syncwarp();
+    };
+
     if (threadIdx.x == 0) mbar_init(bar, 1);
-    if (warp == 0) take_item(a.work_counter, a.items_off, a.F, n_items, nullptr, 0, slots, lane);
+    if (warp == kCtl) {
+        take(&rec[0]);
+        table(&rec[0], ptab);
+        take(&rec[1]);
+    }
     __syncthreads();
     uint32_t phase = 0;
+    int cur = 0;
     Acc acc;
-    const uint32_t F = a.F;
-    const uint64_t *pR = a.pstart, *pS = a.pstart + (F + 1);
 
     while (true) {
-        const uint32_t item = slots[0];
-        if (item >= n_items) break;
-        const uint32_t p = slots[1];
-        const uint64_t r0 = pR[p], nrp = pR[p + 1] - r0;
-        const uint64_t s0 = pS[p], nsp = pS[p + 1] - s0;
-        const uint32_t sch = (uint32_t)((nsp + kSmjSPages - 1) / kSmjSPages);
-        const uint32_t local = item - a.items_off[p];
-        const uint32_t rc = local / sch, sc = local % sch;
-        const uint32_t cid = a.chunk_off[p] + rc;
-        const uint64_t rb = a.cstart[cid];
-        const uint64_t re = rc + 1 < a.chunk_off[p + 1] - a.chunk_off[p] ? a.cstart[cid + 1] : r0 + nrp;
-        const uint32_t nrpg = (uint32_t)(re - rb);
-        const uint64_t sb = s0 + (uint64_t)sc * kSmjSPages;
-        const uint32_t nspg = (uint32_t)min((uint64_t)kSmjSPages, nsp - (uint64_t)sc * kSmjSPages);
+        const SmjRec cr = rec[cur];
+        if (cr.item >= n_items) break;
+        const uint32_t *tpg = ptab + cur * 2 * kSmjTabEntries;
+        const uint32_t *tpk = tpg + kSmjTabEntries;
+        const uint32_t nrpg = cr.nrpg, np = cr.nrpg + cr.nspg;
+        const uint32_t rslots = cr.rslots, sslots = cr.sslots, rpad = cr.rpad, spad = cr.spad;
 
         // --- R chunk -> A and S block -> C, one bulk copy per page, page slots
         //     16-byte aligned (a page takes its count rounded up to even); the
         //     pad slot behind an odd page is set to the all-ones word afterwards,
         //     which sorts last and is cut off by count
-        uint32_t rslots, sslots, rpad, spad;
-        {
-            const uint32_t k = threadIdx.x;   // one page per thread: R pages, then S pages
-            const bool isr = k < nrpg, iss = !isr && k < nrpg + nspg;
-            uint32_t c = 0;
-            if (isr) c = a.Rcount[a.Rlist[rb + k]];
-            else if (iss) c = a.Scount[a.Slist[sb + (k - nrpg)]];
-            const uint32_t e = (c + 1) & ~1u;
-            uint32_t tot;
-            const uint32_t ex = block_exclusive_scan(isr ? e : (e << 16), slots + 4, &tot);   // R | S << 16
-            rslots = tot & 0xFFFFu;
-            sslots = tot >> 16;
-            if (isr) { pdst[k] = ex & 0xFFFFu; pcnt[k] = c; }
-            if (iss) { sdst[k - nrpg] = (ex >> 16); scnt[k - nrpg] = c; }
-            if (threadIdx.x == 0) {
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                mbar_expect_tx(bar, (rslots + sslots) * 8);
-            }
-            rpad = __syncthreads_count(isr && (c & 1));
-            spad = __syncthreads_count(iss && (c & 1));
-        }
-        for (uint32_t k = threadIdx.x; k < nrpg + nspg; k += blockDim.x) {
-            const bool isr = k < nrpg;
-            const uint32_t kk = isr ? k : k - nrpg;
-            const uint32_t c = isr ? pcnt[kk] : scnt[kk];
+        for (uint32_t k = threadIdx.x; k < np; k += blockDim.x) {
+            const uint32_t v = tpk[k], c = v & 0xFFu;
             if (c) {
-                const uint32_t pg = isr ? a.Rlist[rb + kk] : a.Slist[sb + kk];
+                const bool isr = k < nrpg;
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                bulk_g2s(isr ? A + pdst[kk] : C + sdst[kk], (isr ? a.Rpages : a.Spages) + (uint64_t)pg * kPageTuples,
+                bulk_g2s((isr ? A : C) + (v >> 8), (isr ? a.Rpages : a.Spages) + (uint64_t)tpg[k] * kPageTuples,
                          ((c + 1) & ~1u) * 8, bar);
             }
         }
         if (!mbar_wait(bar, phase)) atomicExch(a.err, 1);
         phase ^= 1;
         __syncthreads();
-        for (uint32_t k = threadIdx.x; k < nrpg + nspg; k += blockDim.x) {
-            const bool isr = k < nrpg;
-            const uint32_t kk = isr ? k : k - nrpg;
-            const uint32_t c = isr ? pcnt[kk] : scnt[kk];
-            if (c & 1) (isr ? A + pdst[kk] : C + sdst[kk])[c] = ~0ULL;
+        for (uint32_t k = threadIdx.x; k < np; k += blockDim.x) {
+            const uint32_t v = tpk[k], c = v & 0xFFu;
+            if (c & 1) (k < nrpg ? A : C)[(v >> 8) + c] = ~0ULL;
         }
         __syncthreads();
         // sorted R (+ pads) in B, sorted S (+ pads) in A; the pads are the last
@@ -152,8 +208,13 @@ smj_items(SmjArgs a) {
         const uint32_t nr = rslots - rpad, ns = sslots - spad;
         const uint64_t *Rs = B, *Ss = A;
 
-        // --- merge-join of the sorted runs; warp 0 first takes the next item
-        if (warp == 0) take_item(a.work_counter, a.items_off, F, n_items, nullptr, 0, slots, lane);
+        // --- merge-join of the sorted runs by warps 0 .. 30; the control warp
+        //     prepares the next item and takes the one after it (rec[cur] is
+        //     free: every thread copied it at the top of the item)
+        if (warp == kCtl) {
+            table(&rec[cur ^ 1], ptab + (cur ^ 1) * 2 * kSmjTabEntries);
+            take(&rec[cur]);
+        }
         auto emit = [&](uint64_t s, uint64_t r, uint64_t &sh, bool &have) {
             const uint32_t key = tkey(s);
             if (!have) { sh = s_half(key, tpay(s)); have = true; }
@@ -165,14 +226,14 @@ smj_items(SmjArgs a) {
             }
         };
         // all-ones words beyond the pads: real tuples with key 0xFFFFFFFF
-        const bool ones = !ds.bitonic && (rslots - (ds.nb ? cnt[ds.nb - 1] : 0u) != rpad ||
-                                          sslots - (ds.nb ? cnt[2 * ds.nb] : 0u) != spad);
+        const bool ones = !ds.bitonic && (rslots - (ds.nb ? ds.ex[ds.nb - 1] : 0u) != rpad ||
+                                          sslots - (ds.nb ? ds.ey[ds.nb - 1] : 0u) != spad);
         if (!ds.bitonic && !ds.max_key && !ones) {
             // both runs are ordered by the same buckets: S bucket d meets R bucket
-            // d, whose sorted range [cnt[d - 1], cnt[d]) holds every R tuple that
+            // d, whose sorted range [ex[d - 1], ex[d]) holds every R tuple that
             // can have the S tuple's key; no key is 0xFFFFFFFF, so no pad matches
-            const uint32_t *cx = cnt;
-            for (uint32_t j = threadIdx.x; j < ns; j += blockDim.x) {
+            const uint16_t *cx = ds.ex;
+            for (uint32_t j = threadIdx.x; j < ns && warp != kCtl; j += kWork) {
                 const uint64_t s = Ss[j];
                 const uint32_t key = tkey(s);
                 const uint32_t d = ds.bucket(s);
@@ -184,10 +245,10 @@ smj_items(SmjArgs a) {
                     if (tkey(r) == key) emit(s, r, sh, have);
                 }
             }
-        } else {
+        } else if (warp != kCtl) {
             // merge path over the whole runs; R first on equal keys
             const uint32_t total = nr + ns;
-            const uint32_t L = (total + blockDim.x - 1) / blockDim.x;
+            const uint32_t L = (total + kWork - 1) / kWork;
             const uint32_t k0 = min(total, threadIdx.x * L), k1 = min(total, k0 + L);
             uint32_t lo = k0 > ns ? k0 - ns : 0u, hi = k0 < nr ? k0 : nr;
             while (lo < hi) {   // number of R tuples among the first k0 merged
@@ -208,7 +269,8 @@ smj_items(SmjArgs a) {
                 }
             }
         }
-        __syncthreads();
+        __syncthreads();   // the next item overwrites the buffers; rec / page tables published
+        cur ^= 1;
     }
     block_flush(acc, a.acc, red);
 }

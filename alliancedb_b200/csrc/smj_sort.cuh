@@ -128,7 +128,11 @@ __device__ __forceinline__ void chunk_sort(const uint64_t *src, uint32_t n, uint
 }
 
 
-constexpr uint32_t kDualBucketBits = 11;
+constexpr uint32_t kDualBucketBits = 12;
+
+// Shared-memory words of dual_chunk_sort's counters: two sides of 2^12 + 1
+// 16-bit counters each, packed two per 32-bit word.
+constexpr uint32_t kDualCntWords = ((1u << kDualBucketBits) + 2);
 
 // Insertion sort of dst[b..e) by whole word (one thread).
 __device__ __forceinline__ void insertion_words(uint64_t *dst, uint32_t b, uint32_t e) {
@@ -148,17 +152,30 @@ struct DualSort {
     uint32_t shift, bmask, nb;   // bucket(v) = v == ~0 ? nb : (key >> shift) & bmask
     bool bitonic;                // a side took the bitonic path: bucket ends are not valid
     bool max_key;                // a word other than all-ones has key 0xFFFFFFFF
+    const uint16_t *ex, *ey;     // end of bucket d of Xo / Yo: ex[d], ey[d] (unless bitonic)
     __device__ __forceinline__ uint32_t bucket(uint64_t v) const {
         return v == ~0ULL ? nb : (tkey(v) >> shift) & bmask;
     }
 };
 
+// Adds 1 to 16-bit counter d of a packed array and returns its old value
+// (counts stay below 2^16: a chunk holds at most 8192 words).
+__device__ __forceinline__ uint32_t inc16(uint32_t *w, uint32_t d) {
+    const uint32_t sh = (d & 1u) << 4;
+    return (atomicAdd(&w[d >> 1], 1u << sh) >> sh) & 0xFFFFu;
+}
+
 // chunk_sort of two chunks at once with one bucket function: X[0..nx) -> Xo
-// and Y[0..ny) -> Yo, in the same order rules, with about half the barriers
-// of two calls.  Yo may be X's buffer (X is consumed first); Xo, X and Y must
-// be distinct.  cnt holds 2 * (2^11 + 2) counters: afterwards cnt[d] /
-// cnt[nb + 1 + d] is the end of bucket d of Xo / Yo (unless bitonic).  red
-// holds 96 scratch words.
+// and Y[0..ny) -> Yo (nx, ny <= 8192), in the same order rules, with about half
+// the barriers of two calls.  Yo may be X's buffer (X is consumed first); Xo, X
+// and Y must be distinct.  cnt holds kDualCntWords words: afterwards the result's
+// ex[d] / ey[d] is the end of bucket d of Xo / Yo (unless bitonic).  red holds
+// 96 scratch words.
+//
+// The buckets are the (at most) 12 highest key bits that differ within the two
+// chunks.  When no lower key bit differs, every bucket holds one key value and
+// needs no further order (ties stay in arbitrary order, which merge_join does
+// not depend on), except for payload order among key 0xFFFFFFFF tuples.
 __device__ __forceinline__ DualSort dual_chunk_sort(const uint64_t *X, uint32_t nx, uint64_t *Xo, const uint64_t *Y,
                                                     uint32_t ny, uint64_t *Yo, uint32_t *cnt, uint32_t *red) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -179,6 +196,7 @@ __device__ __forceinline__ DualSort dual_chunk_sort(const uint64_t *X, uint32_t 
         mk |= __shfl_xor_sync(0xffffffffu, mk, s);
     }
     if (lane == 0) { red[wid] = a; red[32 + wid] = o; red[64 + wid] = mk; }
+    for (uint32_t d = threadIdx.x; d < kDualCntWords; d += blockDim.x) cnt[d] = 0;
     __syncthreads();
     a = lane < nw ? red[lane] : 0xFFFFFFFFu;
     o = lane < nw ? red[32 + lane] : 0u;
@@ -198,48 +216,53 @@ __device__ __forceinline__ DualSort dual_chunk_sort(const uint64_t *X, uint32_t 
     r.bmask = r.nb - 1;
     r.max_key = mk != 0;
     const uint32_t nb = r.nb, W = nb + 1;   // counters per side; [nb] = all-ones words
-    uint32_t *cx = cnt, *cy = cnt + W;
-    for (uint32_t d = threadIdx.x; d < 2 * W; d += blockDim.x) cnt[d] = 0;
-    __syncthreads();   // also: every thread has read red
+    uint32_t *wx = cnt, *wy = cnt + (W + 1) / 2;   // packed counter words of each side
+    uint16_t *cx = reinterpret_cast<uint16_t *>(wx), *cy = reinterpret_cast<uint16_t *>(wy);
+    r.ex = cx;
+    r.ey = cy;
     for (uint32_t i = threadIdx.x; i < nx + ny; i += blockDim.x) {
-        if (i < nx) atomicAdd(&cx[r.bucket(X[i])], 1u);
-        else atomicAdd(&cy[r.bucket(Y[i - nx])], 1u);
+        if (i < nx) inc16(wx, r.bucket(X[i]));
+        else inc16(wy, r.bucket(Y[i - nx]));
     }
-    __syncthreads();
-    {   // one exclusive scan over cx then cy; cy's offsets restart at 0 (cx totals nx)
+    __syncthreads();   // also: every thread has read red
+    {   // exclusive scans of both sides' counters, contiguous counters per thread
         const uint32_t per = (2 * W + blockDim.x - 1) / blockDim.x;
         const uint32_t d0 = threadIdx.x * per, d1 = min(2 * W, d0 + per);
         uint32_t loc = 0;
-        for (uint32_t d = d0; d < d1; d++) loc += cnt[d];
+        for (uint32_t d = d0; d < d1; d++) loc += d < W ? cx[d] : cy[d - W];
         uint32_t tot;
         uint32_t ex = block_exclusive_scan(loc, red, &tot);
         for (uint32_t d = d0; d < d1; d++) {
-            const uint32_t c = cnt[d];
-            cnt[d] = d < W ? ex : ex - nx;
-            ex += c;
+            uint16_t &c = d < W ? cx[d] : cy[d - W];
+            const uint32_t v = c;
+            c = (uint16_t)(d < W ? ex : ex - nx);
+            ex += v;
         }
     }
     __syncthreads();
     // X first: Yo may be X's own buffer
     for (uint32_t i = threadIdx.x; i < nx; i += blockDim.x) {
         const uint64_t v = X[i];
-        Xo[atomicAdd(&cx[r.bucket(v)], 1u)] = v;
+        Xo[inc16(wx, r.bucket(v))] = v;
     }
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < ny; i += blockDim.x) {
         const uint64_t v = Y[i];
-        Yo[atomicAdd(&cy[r.bucket(v)], 1u)] = v;
+        Yo[inc16(wy, r.bucket(v))] = v;
     }
     __syncthreads();
-    // cx / cy[d] = end of bucket d; which buckets need whole-word order: see chunk_sort
-    const uint32_t d_first = r.shift == 0 ? ((a | r.bmask) == 0xFFFFFFFFu ? r.bmask : nb) : 0u;
+    // cx / cy[d] = end of bucket d.  Buckets that need whole-word order: all of
+    // them when lower key bits vary; else only the bucket that can hold key
+    // 0xFFFFFFFF (the last one, if every key bit outside the buckets is one).
+    const bool single = (vary & ((1u << r.shift) - 1u)) == 0;
+    const uint32_t d_first = single ? ((a | (r.bmask << r.shift)) == 0xFFFFFFFFu ? r.bmask : nb) : 0u;
     int big = 0;
     for (uint32_t d = d_first + threadIdx.x; d < nb; d += blockDim.x) {
         if (cx[d] - (d ? cx[d - 1] : 0u) > 128) big |= 1;
         if (cy[d] - (d ? cy[d - 1] : 0u) > 128) big |= 2;
     }
     const int bigx = __syncthreads_or(big & 1), bigy = __syncthreads_or(big & 2);
-    if (!bigx || !bigy) {
+    if ((!bigx || !bigy) && d_first < nb) {
         const uint32_t sides = (bigx ? 0u : 1u) | (bigy ? 0u : 2u);
         for (uint32_t t = d_first + threadIdx.x; t < 2 * nb; t += blockDim.x) {
             if (t < nb) {
