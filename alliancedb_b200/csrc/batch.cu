@@ -234,7 +234,7 @@ int batch_launch(Context *ctx, const uint64_t *dR, const uint64_t *r_off, const 
         o.nlog = ctx->ws.take<uint32_t>(G);
         o.plist = ctx->ws.take<uint32_t>(pages);
     }
-    a.df = DigitFn{0u, 0u, 0u};
+    a.df = DigitFn{0u, 0u};
     a.F1 = W;
     a.G = G;
     a.pool_cap = pool_cap;

@@ -173,7 +173,7 @@ partition_pass(PassArgs a) {
         } else {
             b = in.seg_off[p1] + (uint64_t)(g - in.uoff[p1]) * a.unit_tuples;
             e = min(in.seg_off[p1 + 1], b + a.unit_tuples);
-            df = DigitFn{0u, 0u, (1u << in.seg_bits[p1]) - 1u};
+            df = DigitFn{0u, (1u << in.seg_bits[p1]) - 1u};
         }
     }
     const uint32_t F = df.mask + 1;
@@ -287,61 +287,100 @@ partition_pass(PassArgs a) {
             if (k & 1) rk[k / 2] |= r << 16; else rk[k / 2] = r;
         }
         __syncthreads();
-        // B. digit runs of the tile, pages, stream positions: warp w < F / 32
-        //    handles digits 32w .. 32w + 31, one per lane; the warps' totals are
-        //    combined through shared memory (one extra barrier when F > 32)
-        {
+        // B. digit runs of the tile, pages, stream positions.  Up to 128 digits
+        //    warp 0 alone (lane l: digits l*q .. l*q + q - 1, q = F / 32), above
+        //    that warp w < F / 32 takes digits 32w .. 32w + 31, one per lane, and
+        //    the warps' totals are combined through shared memory (one extra
+        //    barrier).  New pages get their log entry in D, from the thread that
+        //    writes their first slot.
+        auto run_digit = [&](uint32_t d, uint32_t L, uint32_t p, uint32_t off, uint32_t first) {
+            const uint32_t room = p == kNone ? 0u : kPageTuples - (p & (kPageTuples - 1));
+            c[d] = 0;
+            toff[d] = off;
+            lim[d] = off + (L < room ? L : room);
+            b1[d] = p - off;
+            uint32_t np = p + L;
+            if (L > room) {
+                const uint32_t need = (L - room + kPageTuples - 1) / kPageTuples;
+                if (first + need > pool_cap) {   // cannot happen: the pool covers the input
+                    atomicExch(a.err, 3);
+                    first = pool_cap - need;
+                }
+                const uint32_t nx = (pool_base + first) * kPageTuples - room;
+                b2[d] = nx - off;
+                np = nx + L;
+            }
+            if (L && (np & (kPageTuples - 1)) == 0) np = kNone;   // page exactly full
+            npos[d] = np;
+        };
+        auto pages_for = [&](uint32_t L, uint32_t p) {
+            const uint32_t room = p == kNone ? 0u : kPageTuples - (p & (kPageTuples - 1));
+            return L > room ? (L - room + kPageTuples - 1) / kPageTuples : 0u;
+        };
+        if (F <= 128) {
+            constexpr int kQ = 4;
+            const uint32_t q = (F + 31) / 32;
+            if (tid < 32) {
+                uint32_t Ls[kQ], Ps[kQ], sumL = 0, sumN = 0;
+#pragma unroll
+                for (int j = 0; j < kQ; j++) {
+                    const uint32_t d = (uint32_t)lane * q + j;
+                    Ls[j] = 0;
+                    Ps[j] = kNone;
+                    if ((uint32_t)j < q && d < F) {
+                        Ls[j] = c[d];
+                        Ps[j] = npos[d];
+                        sumL += Ls[j];
+                        sumN += pages_for(Ls[j], Ps[j]);
+                    }
+                }
+                const uint32_t v = sumL | (sumN << 16);   // L <= kPTile, pages < 2^16
+                const uint32_t inc = warp_incl_scan(v, lane);
+                const uint32_t all = __shfl_sync(0xffffffffu, inc, 31);
+                const uint32_t pool0 = misc[0];
+                uint32_t off = (inc - v) & 0xFFFFu, first = pool0 + ((inc - v) >> 16);
+#pragma unroll
+                for (int j = 0; j < kQ; j++) {
+                    const uint32_t d = (uint32_t)lane * q + j;
+                    if ((uint32_t)j < q && d < F) {
+                        run_digit(d, Ls[j], Ps[j], off, first);
+                        off += Ls[j];
+                        first += pages_for(Ls[j], Ps[j]);
+                    }
+                }
+                __syncwarp();
+                if (lane == 0) {
+                    misc[0] = pool0 + (all >> 16);
+                    misc[1] = all & 0xFFFFu;
+                }
+            }
+        } else {
             const uint32_t nbw = (F + 31) / 32;                 // B warps
             const int bw = tid >> 5;
             const uint32_t d = (uint32_t)tid;                   // this lane's digit
-            uint32_t L = 0, p = kNone, room = 0, need = 0, inc = 0, pool0 = 0;
+            uint32_t L = 0, p = kNone, need = 0, inc = 0, pool0 = 0;
             if (bw < (int)nbw) {
                 if (d < F) {
                     L = c[d];
                     p = npos[d];
-                    room = p == kNone ? 0u : kPageTuples - (p & (kPageTuples - 1));
-                    need = L > room ? (L - room + kPageTuples - 1) / kPageTuples : 0u;
+                    need = pages_for(L, p);
                 }
                 inc = warp_incl_scan(L | (need << 16), lane);   // L <= kPTile, pages of 32 digits < 2^16
                 pool0 = misc[0];
-                if (nbw > 1 && lane == 31) misc[8 + bw] = inc;
+                if (lane == 31) misc[8 + bw] = inc;
             }
-            if (nbw > 1) __syncthreads();   // every B warp has read misc[0] and written its total
+            __syncthreads();   // every B warp has read misc[0] and written its total
             if (bw < (int)nbw) {
                 // totals of the warps before this one, and of all of them
-                const uint32_t own = __shfl_sync(0xffffffffu, inc, 31);
                 uint32_t before_t = 0, before_p = 0, all_t = 0, all_p = 0;
                 for (uint32_t k = 0; k < nbw; k++) {
-                    const uint32_t tv = nbw > 1 ? misc[8 + k] : own;
+                    const uint32_t tv = misc[8 + k];
                     if ((int)k < bw) { before_t += tv & 0xFFFFu; before_p += tv >> 16; }
                     all_t += tv & 0xFFFFu;
                     all_p += tv >> 16;
                 }
                 const uint32_t ex = inc - (L | (need << 16));
-                if (d < F) {
-                    const uint32_t off = before_t + (ex & 0xFFFFu);
-                    c[d] = 0;
-                    toff[d] = off;
-                    lim[d] = off + (L < room ? L : room);
-                    b1[d] = p - off;
-                    uint32_t np = p + L;
-                    if (need) {
-                        uint32_t first = pool0 + before_p + (ex >> 16);
-                        if (first + need > pool_cap) {   // cannot happen: the pool covers the input
-                            atomicExch(a.err, 3);
-                            first = pool_cap - need;
-                        }
-                        for (uint32_t k = 0; k < need; k++) {
-                            o.log[pool_base + first + k] = dbase + d;
-                            o.pcount[pool_base + first + k] = kPageTuples;
-                        }
-                        const uint32_t nx = (pool_base + first) * kPageTuples - room;
-                        b2[d] = nx - off;
-                        np = nx + L;
-                    }
-                    if (L && (np & (kPageTuples - 1)) == 0) np = kNone;   // page exactly full
-                    npos[d] = np;
-                }
+                if (d < F) run_digit(d, L, p, before_t + (ex & 0xFFFFu), pool0 + before_p + (ex >> 16));
                 if (bw == 0 && lane == 0) {   // warp 0 read misc[0] before the shuffle above
                     misc[0] = pool0 + all_p;
                     misc[1] = all_t;
@@ -366,6 +405,10 @@ partition_pass(PassArgs a) {
             const uint32_t d = df(tkey(v));
             const uint32_t dst = i + (i < lim[d] ? b1[d] : b2[d]);
             o.pages[dst] = v;
+            if ((dst & (kPageTuples - 1)) == 0) {   // first slot of a page taken in B
+                o.log[dst / kPageTuples] = dbase + d;
+                o.pcount[dst / kPageTuples] = kPageTuples;
+            }
         }
         // the next tile's A uses the other counter array and registers only;
         // its B / C run after the next barrier, when every thread is past D

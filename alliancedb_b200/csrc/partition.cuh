@@ -1,9 +1,11 @@
 // partition.cuh -- digit functions and the small scans shared by the
 // partitioned joins (paged.cuh does the partitioning itself).
-// The digit is ((key - kmin) >> shift) & (F - 1): shift 0 / kmin 0 is the low-bit
-// radix of PRO (HASH_BIT_MODULO, hashing/joins/parallel_radix_join.cpp:68); a
-// range partition for the sort-merge join uses the high bits of key - kmin
-// (the MSB radix of sorting/joins/sortmergejoin_multiway.cpp:475-487).
+// The digit is (key >> shift) & (F - 1): the low-bit radix of PRO
+// (HASH_BIT_MODULO, hashing/joins/parallel_radix_join.cpp:68), shift = the bits
+// an earlier pass consumed.  The sort-merge joins partition on the same low
+// bits (equal keys still meet in one partition; the reference's range split of
+// the high bits, sorting/joins/sortmergejoin_multiway.cpp:475-487, is not needed
+// for that).
 #pragma once
 
 #include "adb_common.cuh"
@@ -20,12 +22,9 @@ __device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
 }
 
 struct DigitFn {
-    uint32_t kmin;
     uint32_t shift;
     uint32_t mask;      // F - 1
-    __host__ __device__ __forceinline__ uint32_t operator()(uint32_t key) const {
-        return ((key - kmin) >> shift) & mask;
-    }
+    __host__ __device__ __forceinline__ uint32_t operator()(uint32_t key) const { return (key >> shift) & mask; }
 };
 
 struct RelPair {

@@ -233,8 +233,8 @@ int run_radix(Context *ctx, const DevJoin &j, bool hist_table, int bits, unsigne
     cudaStream_t st = ctx->stream;
     uint32_t b1, b2;
     split_bits(bits, &b1, &b2);
-    const DigitFn d1{0u, 0u, (1u << b1) - 1};
-    const DigitFn d2{0u, b1, (1u << b2) - 1};
+    const DigitFn d1{0u, (1u << b1) - 1};
+    const DigitFn d2{b1, (1u << b2) - 1};
     PartOut po;
     ADB_TRY(run_paged_partition(ctx, j, d1, b2 ? &d2 : nullptr, &po, acc));
     ADB_CK(cudaEventRecord(ctx->ev[2], st));   // phases: pass 1 | pass 2 | work list | join
