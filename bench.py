@@ -48,15 +48,18 @@ ALG_BYTES = {"PRO": 24, "RJ_st": 24, "PRH": 24, "PRHO": 24, "NPO": 16, "NPO_st":
 # Per family: phase index (adb_join_result.ms_phase) -> (kernel, algorithmic
 # bytes per input tuple of one launch, DRAM bytes per input tuple of one launch
 # measured by ncu on |R| = |S| = 2^24 (profiles/partition_pass_pro_2e24.md,
-# profiles/radix_join_items_pro_2e24.md), None where not captured).  The
-# traffic of a full-size launch is that figure times the launch's tuples: both
-# kernels stream every tuple once, so traffic grows in proportion.
+# profiles/radix_join_items_pro_2e24.md, profiles/smj_items_mway_2e24.md), None
+# where not captured).  The traffic of a full-size launch is that figure times
+# the launch's tuples: the kernels stream every tuple once, so traffic grows in
+# proportion.
 KERNELS = {
-    "radix": {0: ("partition_pass<0,512> (pass 1)", 16, (269997824 + 229477888) / 2**25),
-              1: ("partition_pass<1,512> (pass 2)", 16, (273354240 + 226931200) / 2**25),
-              3: ("radix_join_items<Chain>", 8, (273622528 + 4446208) / 2**25)},
+    "radix": {0: ("partition_pass<0,512> (pass 1)", 16, (270285568 + 214802176) / 2**25),
+              1: ("partition_pass<1,512> (pass 2)", 16, (273331456 + 214424576) / 2**25),
+              3: ("radix_join_items<Chain>", 8, (273641984 + 7539456) / 2**25)},
     "npo": {0: ("npo_build", 8, None), 3: ("npo_probe", 8, None)},
-    "smj": {0: ("partition_pass (all passes)", 16, None), 3: ("smj_items", 8, None)},
+    "smj": {0: ("partition_pass (both passes)", 32,
+                (271129856 + 214481152 + 275816192 + 215750912) / 2**25),
+            3: ("smj_items", 8, (276513536 + 4389632) / 2**25)},
 }
 
 
