@@ -147,6 +147,7 @@ _SIGS = {
     "adb_gen_pk": (C.c_int, [_P, _U64, _U64, C.c_int]),
     "adb_gen_fk": (C.c_int, [_P, _U64, _P, _U64, C.c_double, _U64, _P, C.c_int]),
     "adb_gen_uniform": (C.c_int, [_P, _U64, _U64, _U64, C.c_int]),
+    "adb_load_relation": (C.c_int, [C.c_char_p, C.c_int32, C.c_int32, C.c_uint32, _U64, _P, _P]),
 }
 
 
@@ -346,6 +347,17 @@ class DeviceBuffer:
 
 
 # ---- generators (host) ----
+def load_relation(path: str, num_tuples: int, key_col: int = 0, ts_col: int = 0, partitions: int = 1):
+    """Relation of num_tuples records from a ',' or '|' separated text file, as
+    the reference's file loader reads it (adb_load_relation): returns
+    (tuples, timestamps); the timestamps are 0 when ts_col is 0."""
+    t = np.empty(num_tuples, dtype=TUPLE)
+    ts = np.empty(num_tuples, dtype=np.uint64)
+    _check(lib().adb_load_relation(str(path).encode(), key_col, ts_col, partitions, num_tuples,
+                                   t.ctypes.data if num_tuples else None, ts.ctypes.data if num_tuples else None))
+    return t, ts
+
+
 def gen_pk(n: int, seed: int) -> np.ndarray:
     out = np.empty(n, dtype=TUPLE)
     _check(lib().adb_gen_pk(out.ctypes.data if n else None, n, seed, 0))

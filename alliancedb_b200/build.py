@@ -73,7 +73,7 @@ def build_oracle() -> Path:
     present on this machine) the reference's own joins under oracle/_ref/."""
     _run(["make", "-s", "-C", str(ROOT / "oracle"), "liboracle.so"])
     if REF_SRC.is_dir():
-        _run(["make", "-s", "-C", str(ROOT / "oracle"), "ref", f"REF_SRC={REF_SRC}"])
+        _run(["make", "-s", "-C", str(ROOT / "oracle"), "ref", "read", f"REF_SRC={REF_SRC}"])
     return ORACLE_LIB
 
 

@@ -268,6 +268,24 @@ int adb_gen_fk(adb_tuple *S, uint64_t nS, const adb_tuple *R, uint64_t nR, doubl
 /* Non-unique: key = 1 + uniform(seed, i) % key_range, payload = i. */
 int adb_gen_uniform(adb_tuple *T, uint64_t n, uint64_t key_range, uint64_t seed, int on_device);
 
+/* ---------------------------------------------------------------------- */
+/* Relations from text files (host only, no device needed).               */
+/* ---------------------------------------------------------------------- */
+
+/* Reads num_tuples records of the text file at path into tuples (and their
+ * timestamps into ts, which may be NULL), as the reference's file loader does.
+ * Replaces load_relation / read_relation (hashing/utils/generator.cpp:646-666,
+ * :900-1027), called from createRelation (hashing/benchmark.cpp:80-83):
+ * fields separated by the first ',' or '|' of the file, no header line, key =
+ * integer field key_col, timestamp = integer field ts_col (milliseconds) times
+ * 2.1e6 when ts_col != 0 (0 otherwise), runs of equal timestamps spread
+ * linearly to the next one (smooth, :1050-1067), record i placed round-robin
+ * into `partitions` contiguous ranges, payload = its index.  ADB_ERR_ARG when
+ * the file cannot be read, has fewer than num_tuples records, or a record lacks
+ * the fields (the reference's behaviour is undefined there). */
+int adb_load_relation(const char *path, int32_t key_col, int32_t ts_col, uint32_t partitions,
+                      uint64_t num_tuples, adb_tuple *tuples, uint64_t *ts);
+
 #ifdef __cplusplus
 }
 #endif
