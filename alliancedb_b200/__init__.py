@@ -78,6 +78,20 @@ class WindowResult(C.Structure):
     ]
 
 
+class WindowProgress(C.Structure):
+    """adb_window_progress: ms to pct = 1, 5, 10, 25, 50, 75, 95, 99, 100 % of a
+    window's matches, and match-weighted batch latency percentiles (ms)."""
+    PCT = (1, 5, 10, 25, 50, 75, 95, 99, 100)
+    _fields_ = [
+        ("t_pct", C.c_float * 9),
+        ("lat_p50", C.c_float),
+        ("lat_p95", C.c_float),
+        ("lat_p99", C.c_float),
+        ("batches", C.c_uint32),
+        ("reserved", C.c_uint32),
+    ]
+
+
 class ServeRequest(C.Structure):
     _fields_ = [("arrival_us", C.c_uint64), ("n_r", C.c_uint32), ("n_s", C.c_uint32), ("seed", C.c_uint64)]
 
@@ -126,6 +140,9 @@ _SIGS = {
                                   C.POINTER(JoinResult), _P]),
     "adb_join_materialize_device": (C.c_int, [C.c_char_p, _P, _U64, _P, _U64, C.POINTER(JoinParams), _P, _U64,
                                               C.POINTER(JoinResult), _P]),
+    "adb_stream_join_progress": (C.c_int, [C.c_char_p, _P, _U64, _P, _U64, C.POINTER(JoinParams),
+                                           C.POINTER(WindowResult), C.POINTER(WindowProgress), _U64,
+                                           C.POINTER(C.c_uint64)]),
     "adb_stream_join": (C.c_int, [C.c_char_p, _P, _U64, _P, _U64, C.POINTER(JoinParams),
                                   C.POINTER(WindowResult), _U64, C.POINTER(C.c_uint64)]),
     "adb_batch_join_device": (C.c_int, [_P, C.POINTER(C.c_uint64), _P, C.POINTER(C.c_uint64), C.c_uint32,
@@ -254,17 +271,23 @@ def join_materialize_device(algo: str, dR: int, nR: int, dS: int, nS: int, dOut:
 
 
 def stream_join(algo: str, R: np.ndarray, S: np.ndarray, params: JoinParams | None = None,
-                max_windows: int = 1 << 16) -> list[WindowResult]:
-    """Windowed eager join of two timestamp-ordered STREAM_TUPLE arrays."""
+                max_windows: int = 1 << 16, progress: bool = False):
+    """Windowed eager join of two timestamp-ordered STREAM_TUPLE arrays: the
+    per-window results, and with progress=True also their WindowProgress
+    (adb_stream_join_progress) as a second list."""
     R = np.ascontiguousarray(R, dtype=STREAM_TUPLE)
     S = np.ascontiguousarray(S, dtype=STREAM_TUPLE)
     out = (WindowResult * max_windows)()
+    prog = (WindowProgress * max_windows)() if progress else None
     nw = C.c_uint64(0)
-    st = lib().adb_stream_join(algo.encode(), R.ctypes.data if R.size else None, R.size,
-                               S.ctypes.data if S.size else None, S.size,
-                               C.byref(params) if params is not None else None, out, max_windows, C.byref(nw))
+    st = lib().adb_stream_join_progress(algo.encode(), R.ctypes.data if R.size else None, R.size,
+                                        S.ctypes.data if S.size else None, S.size,
+                                        C.byref(params) if params is not None else None, out, prog, max_windows,
+                                        C.byref(nw))
     _check(st)
-    return [out[i] for i in range(min(nw.value, max_windows))]
+    n = min(nw.value, max_windows)
+    wins = [out[i] for i in range(n)]
+    return (wins, [prog[i] for i in range(n)]) if progress else wins
 
 
 def batch_join_device(dR: int, r_off: np.ndarray, dS: int, s_off: np.ndarray, mode: int = 0):

@@ -35,6 +35,7 @@
 //        accumulation.
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <thread>
 #include <vector>
 
@@ -368,9 +369,57 @@ int eager_set_attrs() {
 // ---------------------------------------------------------------------------
 // Timestamped streams in tumbling windows
 // ---------------------------------------------------------------------------
+
+// One thread: out[0] = the device's global nanosecond clock, out[1] = the
+// window's match count so far (when acc is given).  Stream-ordered after (or
+// before) a micro-batch's kernels, it stamps when the batch's results exist.
+static __global__ void stamp_kernel(const unsigned long long *acc, unsigned long long *out) {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    out[0] = t;
+    if (acc) out[1] = acc[0];
+}
+
+// Progress of one window from its per-batch stamps: rel[k] = release time,
+// done[k] = results time (ns), cum[k] = matches after batch k.
+static void window_progress(const std::vector<unsigned long long> &st, uint64_t steps, adb_window_progress *o) {
+    static const double kPct[9] = {1, 5, 10, 25, 50, 75, 95, 99, 100};
+    auto rel = [&](uint64_t k) { return st[3 * k]; };
+    auto done = [&](uint64_t k) { return st[3 * k + 1]; };
+    auto cum = [&](uint64_t k) { return st[3 * k + 2]; };
+    *o = adb_window_progress{};
+    o->batches = (uint32_t)steps;
+    if (!steps) return;
+    const uint64_t total = cum(steps - 1);
+    uint64_t k = 0;
+    for (int i = 0; i < 9; i++) {
+        const uint64_t target = (uint64_t)std::ceil((double)total * kPct[i] / 100.0);
+        while (k + 1 < steps && cum(k) < target) k++;
+        o->t_pct[i] = total ? (float)((double)(done(k) - rel(0)) / 1e6) : 0.f;
+    }
+    // match-weighted latency percentiles of the batches
+    std::vector<std::pair<double, uint64_t>> lat;
+    for (uint64_t b = 0; b < steps; b++) {
+        const uint64_t m = cum(b) - (b ? cum(b - 1) : 0);
+        if (m) lat.emplace_back((double)(done(b) - rel(b)) / 1e6, m);
+    }
+    std::sort(lat.begin(), lat.end());
+    auto pct = [&](double q) {
+        uint64_t seen = 0;
+        for (const auto &x : lat) {
+            seen += x.second;
+            if ((double)seen >= q * (double)total) return (float)x.first;
+        }
+        return lat.empty() ? 0.f : (float)lat.back().first;
+    };
+    o->lat_p50 = pct(0.50);
+    o->lat_p95 = pct(0.95);
+    o->lat_p99 = pct(0.99);
+}
+
 int stream_join(Context *ctx, Family fam, int model, const adb_stream_tuple *R, uint64_t nR,
                 const adb_stream_tuple *S, uint64_t nS, const adb_join_params *p, adb_window_result *out,
-                uint64_t max_windows, uint64_t *n_windows) {
+                adb_window_progress *progress, uint64_t max_windows, uint64_t *n_windows) {
     cudaStream_t st = ctx->stream;
     const uint64_t W = p && p->window_size > 0 ? (uint64_t)p->window_size : 1000;
     const uint64_t batch = p && p->batch_tuples > 0 ? (uint64_t)p->batch_tuples : 1600;
@@ -404,11 +453,29 @@ int stream_join(Context *ctx, Family fam, int model, const adb_stream_tuple *R, 
         capS = std::max(capS, sb[w + 1] - sb[w]);
     }
     const EagerPlan plan = plan_eager(fam, model, nthreads, group_size, capR, capS, std::max(capR, capS));
-    const size_t in_bytes = Workspace::need(nR + 1, 16) + Workspace::need(nS + 1, 16);
+    // micro-batches of window w: SHJ `batch` tuples per side, PMJ progressive_step % runs
+    auto step_sizes = [&](uint64_t w, uint64_t *sr, uint64_t *ss) {
+        *sr = *ss = batch;
+        if (fam == Family::Pmj) {
+            *sr = std::max<uint64_t>(1, (rb[w + 1] - rb[w]) * pstep / 100);
+            *ss = std::max<uint64_t>(1, (sb[w + 1] - sb[w]) * pstep / 100);
+        }
+        return std::max<uint64_t>(1, std::max((rb[w + 1] - rb[w] + *sr - 1) / *sr, (sb[w + 1] - sb[w] + *ss - 1) / *ss));
+    };
+    uint64_t max_steps = 1;
+    if (progress)
+        for (uint64_t w = 0; w < nwin && w < max_windows; w++) {
+            uint64_t a, b;
+            max_steps = std::max(max_steps, step_sizes(w, &a, &b));
+        }
+    const size_t in_bytes = Workspace::need(nR + 1, 16) + Workspace::need(nS + 1, 16) +
+                            (progress ? Workspace::need(3 * max_steps, 8) : 0);
     ADB_TRY(ctx->ws.reserve(in_bytes + eager_plan_bytes(plan) + 4096));
     uint64_t *dR = reinterpret_cast<uint64_t *>(ctx->ws.take<adb_stream_tuple>(nR + 1));
     uint64_t *dS = reinterpret_cast<uint64_t *>(ctx->ws.take<adb_stream_tuple>(nS + 1));
     unsigned long long *acc = ctx->ws.take<unsigned long long>(4);
+    unsigned long long *stamps = progress ? ctx->ws.take<unsigned long long>(3 * max_steps) : nullptr;
+    std::vector<unsigned long long> h_stamps(progress ? 3 * max_steps : 0);
     EagerWindow win;
     take_window(ctx, plan, win);
     if (nR) ADB_CK(cudaMemcpyAsync(dR, R, nR * 16, cudaMemcpyHostToDevice, st));
@@ -420,13 +487,9 @@ int stream_join(Context *ctx, Family fam, int model, const adb_stream_tuple *R, 
         const uint64_t r0 = rb[w], r1 = rb[w + 1], s0 = sb[w], s1 = sb[w + 1];
         ADB_TRY(reset_window(ctx, plan, win));
         ADB_CK(cudaMemsetAsync(acc, 0, 32, st));
-        // micro-batches: SHJ `batch` tuples per side, PMJ progressive_step % runs
-        uint64_t sr = batch, ss = batch;
-        if (fam == Family::Pmj) {
-            sr = std::max<uint64_t>(1, (r1 - r0) * pstep / 100);
-            ss = std::max<uint64_t>(1, (s1 - s0) * pstep / 100);
-        }
-        const uint64_t steps = std::max<uint64_t>(1, std::max((r1 - r0 + sr - 1) / sr, (s1 - s0 + ss - 1) / ss));
+        uint64_t sr, ss;
+        const uint64_t steps = step_sizes(w, &sr, &ss);
+        const bool stamp = progress && w < max_windows;
         for (uint64_t k = 0; k < steps; k++) {
             const uint64_t a0 = std::min(r1, r0 + k * sr), a1 = k + 1 == steps ? r1 : std::min(r1, r0 + (k + 1) * sr);
             const uint64_t c0 = std::min(s1, s0 + k * ss), c1 = k + 1 == steps ? s1 : std::min(s1, s0 + (k + 1) * ss);
@@ -439,8 +502,14 @@ int stream_join(Context *ctx, Family fam, int model, const adb_stream_tuple *R, 
                 std::this_thread::sleep_until(due);
             }
             if (k + 1 == steps) ADB_CK(cudaEventRecord(ctx->ev[4], st));
+            if (stamp) stamp_kernel<<<1, 1, 0, st>>>(nullptr, stamps + 3 * k);
             ADB_TRY(eager_step(ctx, plan, win, dR + 2 * a0, a1 - a0, dS + 2 * c0, c1 - c0, 2, acc));
+            if (stamp) {
+                stamp_kernel<<<1, 1, 0, st>>>(acc, stamps + 3 * k + 1);
+                ctx->kernels += 2;
+            }
         }
+        if (stamp) ADB_CK(cudaMemcpyAsync(h_stamps.data(), stamps, 3 * steps * 8, cudaMemcpyDeviceToHost, st));
         const auto close = std::chrono::steady_clock::now();
         ADB_CK(cudaMemcpyAsync(ctx->h_res, acc, 32, cudaMemcpyDeviceToHost, st));
         ADB_CK(cudaEventRecord(ctx->ev[5], st));
@@ -464,6 +533,7 @@ int stream_join(Context *ctx, Family fam, int model, const adb_stream_tuple *R, 
             }
             o.latency_ms = ms;
             o.reserved = 0;
+            if (progress) window_progress(h_stamps, steps, &progress[w]);
         }
     }
     *n_windows = nwin;

@@ -412,6 +412,12 @@ int adb_join(const char *algo, const adb_tuple *R, uint64_t nR, const adb_tuple 
 int adb_stream_join(const char *algo, const adb_stream_tuple *R, uint64_t nR, const adb_stream_tuple *S,
                     uint64_t nS, const adb_join_params *p, adb_window_result *windows, uint64_t max_windows,
                     uint64_t *n_windows) {
+    return adb_stream_join_progress(algo, R, nR, S, nS, p, windows, nullptr, max_windows, n_windows);
+}
+
+int adb_stream_join_progress(const char *algo, const adb_stream_tuple *R, uint64_t nR, const adb_stream_tuple *S,
+                             uint64_t nS, const adb_join_params *p, adb_window_result *windows,
+                             adb_window_progress *progress, uint64_t max_windows, uint64_t *n_windows) {
     if (!n_windows) { set_error("n_windows is NULL"); return ADB_ERR_ARG; }
     *n_windows = 0;
     const AlgoEntry *a = find_algo(algo);
@@ -430,7 +436,7 @@ int adb_stream_join(const char *algo, const adb_stream_tuple *R, uint64_t nR, co
     Context *ctx = held_.ctx;
     if (!ctx) return s;
     ctx->kernels = 0;
-    return stream_join(ctx, a->fam, a->model, R, nR, S, nS, p, windows, max_windows, n_windows);
+    return stream_join(ctx, a->fam, a->model, R, nR, S, nS, p, windows, progress, max_windows, n_windows);
 }
 
 int adb_device_alloc(void **ptr, size_t bytes) {

@@ -51,6 +51,6 @@ int run_eager(Context *ctx, const DevJoin &j, Family fam, int model, uint64_t ba
               int group_size, int progressive_step, uint64_t seed, unsigned long long *acc);
 int stream_join(Context *ctx, Family fam, int model, const adb_stream_tuple *R, uint64_t nR,
                 const adb_stream_tuple *S, uint64_t nS, const adb_join_params *p, adb_window_result *out,
-                uint64_t max_windows, uint64_t *n_windows);
+                adb_window_progress *progress, uint64_t max_windows, uint64_t *n_windows);
 
 }  // namespace adb

@@ -150,6 +150,31 @@ int adb_stream_join(const char *algo, const adb_stream_tuple *R, uint64_t nR,
                     const adb_stream_tuple *S, uint64_t nS, const adb_join_params *p,
                     adb_window_result *windows, uint64_t max_windows, uint64_t *n_windows);
 
+/* Progressiveness of one window: the reference's progressive measurement
+ * (END_PROGRESSIVE_MEASURE samples every gap-th match with its time and the
+ * probing tuple, hashing/timer/t_timer.h:195-212; dump_timing reports the time
+ * to 1..50 % of the results and the 95th / 99th tuple latency,
+ * hashing/timer/t_timer.cpp:401-452), taken per arrival micro-batch on the
+ * device clock.  t_pct[i] = ms from the release of the window's first batch
+ * until the results of the batch that brings the window's matches to pct[i] %
+ * of its total, pct = {1, 5, 10, 25, 50, 75, 95, 99, 100}; lat_* = percentiles,
+ * weighted by each batch's matches, of the ms from a batch's release (its
+ * start on the device; with p->realtime, the arrival of its last tuple) to its
+ * results. */
+typedef struct adb_window_progress {
+    float t_pct[9];
+    float lat_p50, lat_p95, lat_p99;
+    uint32_t batches;
+    uint32_t reserved;
+} adb_window_progress;
+
+/* adb_stream_join that also fills progress[w] (may be NULL) for the first
+ * max_windows windows; each micro-batch adds two one-thread clock kernels. */
+int adb_stream_join_progress(const char *algo, const adb_stream_tuple *R, uint64_t nR,
+                             const adb_stream_tuple *S, uint64_t nS, const adb_join_params *p,
+                             adb_window_result *windows, adb_window_progress *progress,
+                             uint64_t max_windows, uint64_t *n_windows);
+
 /* ---------------------------------------------------------------------- */
 /* Batched windows: many independent R/S pairs joined in one launch.      */
 /* ---------------------------------------------------------------------- */

@@ -126,3 +126,28 @@ def test_stream_models_agree():
     for algo in EAGER[1:]:
         got = [(w.count, w.checksum) for w in adb.stream_join(algo, R, S, p)]
         assert got == ref, algo
+
+
+@pytest.mark.parametrize("algo", ["SHJ_JM_NP", "PMJ_JM_NP"])
+@pytest.mark.parametrize("realtime", [0, 1])
+def test_stream_progress(oracle, algo, realtime):
+    """Progressiveness per window (adb_stream_join_progress): results equal the
+    plain call's, the time to k % of the matches grows with k and ends at the
+    last batch, latency percentiles are ordered, and with the arrival schedule
+    (realtime) a 1 ms micro-batch has its results within the window."""
+    R, S = make_streams(6000, 6.0, 1000, 4, 13)      # ~1 s of stream at 6 tuples/ms per side
+    p = adb.default_params(window_size=250, batch_tuples=6, progressive_step=10, realtime=realtime)
+    plain = adb.stream_join(algo, R, S, p)
+    wins, prog = adb.stream_join(algo, R, S, p, progress=True)
+    assert [(w.count, w.checksum) for w in wins] == [(w.count, w.checksum) for w in plain]
+    for w, g in zip(wins, prog):
+        t = list(g.t_pct)
+        assert g.batches >= 1
+        if w.count == 0:
+            assert t == [0.0] * 9
+            continue
+        assert all(a <= b for a, b in zip(t, t[1:])), t
+        assert t[0] >= 0 and g.lat_p50 <= g.lat_p95 <= g.lat_p99
+        if realtime:
+            assert t[-1] < 250 + 50      # the last batch is released near the window's end
+            assert g.lat_p99 < 50        # a batch's results follow its release closely
