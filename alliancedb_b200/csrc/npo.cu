@@ -7,9 +7,10 @@
 
 namespace adb {
 
+// 2 slots per build tuple, at least 4 (one 32-byte sector: the probe reads whole sectors)
 static uint32_t npo_log2(uint64_t nR) {
     uint32_t l = ceil_log2_u64(2 * (nR ? nR : 1));
-    return l < 1 ? 1 : l;
+    return l < 2 ? 2 : l;
 }
 
 size_t npo_scratch(uint64_t nR) {

@@ -47,41 +47,89 @@ static __global__ void npo_build(const uint64_t *__restrict__ R, uint64_t nR, ui
     }
 }
 
+// Probe: each thread takes kProbeU S tuples at a time (a grid-stride group),
+// so that kProbeU random table reads are in flight per thread.  A probe reads
+// the whole 32-byte sector that holds its start slot (two 16-byte loads) and
+// scans it from the start slot; only a probe whose run of occupied slots
+// reaches the sector's end goes on slot by slot, as linear probing does.
+constexpr int kProbeU = 4;
+
 template <bool kMaterialize>
 __global__ void npo_probe(const uint64_t *__restrict__ S, uint64_t nS, const uint64_t *__restrict__ table,
                           uint32_t log2n, const unsigned long long *sentinel_cnt, unsigned long long *acc,
                           uint64_t *mat, unsigned long long *mat_n, uint64_t mat_cap) {
     __shared__ uint64_t red[64];
     const uint64_t mask = (1ULL << log2n) - 1;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t T = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t nsent = *sentinel_cnt;
     Acc a;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nS; i += stride) {
-        const uint64_t s = __ldcs(reinterpret_cast<const unsigned long long *>(S) + i);
-        const uint32_t key = tkey(s);
-        const uint64_t sh = s_half(key, tpay(s));
-        uint64_t slot = npo_hash(key, log2n);
-        for (uint64_t tries = 0; tries <= mask; tries++) {
-            const uint64_t v = table[slot];
-            if (v == kEmpty) break;
-            if (tkey(v) == key) {
-                a.count++;
-                a.sum += pair_hash_pre(key, tpay(v), sh);
-                if (kMaterialize) {
-                    const unsigned long long k = atomicAdd(mat_n, 1ull);
-                    if (k < mat_cap) mat[k] = s;
+    auto match = [&](uint64_t s, uint32_t key, uint32_t rpay, uint64_t sh) {
+        a.count++;
+        a.sum += pair_hash_pre(key, rpay, sh);
+        if (kMaterialize) {
+            const unsigned long long k = atomicAdd(mat_n, 1ull);
+            if (k < mat_cap) mat[k] = s;
+        }
+    };
+    for (uint64_t g0 = tid; g0 < nS; g0 += T * kProbeU) {
+        uint64_t s[kProbeU], slot[kProbeU];
+        ulonglong2 lo[kProbeU], hi[kProbeU];
+        bool ok[kProbeU];
+#pragma unroll
+        for (int u = 0; u < kProbeU; u++) {   // S tuples g0, g0 + T, ...: coalesced across the warp
+            const uint64_t i = g0 + (uint64_t)u * T;
+            ok[u] = i < nS;
+            s[u] = ok[u] ? __ldcs(reinterpret_cast<const unsigned long long *>(S) + i) : 0ULL;
+        }
+#pragma unroll
+        for (int u = 0; u < kProbeU; u++) {   // the sectors: all loads issued before any is used
+            slot[u] = npo_hash(tkey(s[u]), log2n);
+            const ulonglong2 *sec = reinterpret_cast<const ulonglong2 *>(table + (slot[u] & ~3ULL));
+            if (ok[u]) {
+                lo[u] = __ldg(sec);
+                hi[u] = __ldg(sec + 1);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kProbeU; u++) {
+            if (!ok[u]) continue;
+            const uint32_t key = tkey(s[u]);
+            const uint64_t sh = s_half(key, tpay(s[u]));
+            const uint64_t w4[4] = {lo[u].x, lo[u].y, hi[u].x, hi[u].y};
+            bool open = true;   // no empty slot met yet
+            uint32_t hits = 0;  // matching slots of the sector
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                if (open && (uint64_t)j >= (slot[u] & 3)) {
+                    if (w4[j] == kEmpty) open = false;
+                    else if (tkey(w4[j]) == key) hits |= 1u << j;
                 }
             }
-            slot = (slot + 1) & mask;
-        }
-        if (key == 0xFFFFFFFFu && nsent) {
-            a.count += nsent;
-            a.sum += nsent * pair_hash_pre(key, 0xFFFFFFFFu, sh);
-            if (kMaterialize)
-                for (uint64_t t = 0; t < nsent; t++) {
-                    const unsigned long long k = atomicAdd(mat_n, 1ull);
-                    if (k < mat_cap) mat[k] = s;
+            while (hits) {       // one call site for the checksum (usually one match)
+                const int j = __ffs(hits) - 1;
+                hits &= hits - 1;
+                const ulonglong2 h2 = j & 2 ? hi[u] : lo[u];
+                match(s[u], key, tpay(j & 1 ? h2.y : h2.x), sh);
+            }
+            if (open) {   // the run reaches the sector's end: continue linear probing
+                uint64_t sl = ((slot[u] & ~3ULL) + 4) & mask;
+                for (uint64_t tries = 0; tries <= mask; tries++) {
+                    const uint64_t v = table[sl];
+                    if (v == kEmpty) break;
+                    if (tkey(v) == key) match(s[u], key, tpay(v), sh);
+                    sl = (sl + 1) & mask;
                 }
+            }
+            if (key == 0xFFFFFFFFu && nsent) {
+                a.count += nsent;
+                a.sum += nsent * pair_hash_pre(key, 0xFFFFFFFFu, sh);
+                if (kMaterialize)
+                    for (uint64_t t = 0; t < nsent; t++) {
+                        const unsigned long long k = atomicAdd(mat_n, 1ull);
+                        if (k < mat_cap) mat[k] = s[u];
+                    }
+            }
         }
     }
     block_flush(a, acc, red);
