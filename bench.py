@@ -371,6 +371,10 @@ def main():
                      "pipeline": {"alg_bytes_per_tuple": ALG_BYTES.get(args.algo, 24), "achieved": pipe_gbs,
                                   "frac": pipe_gbs / hbm}},
         "phases_ms": [float(x) for x in ph],
+        **({"random_access": {
+            "note": "NPO's table (2 slots per R tuple) is far larger than L2: every insert and probe is a random "
+                    "32-byte DRAM access, so its bound is the random access rate, not sequential bandwidth",
+            "build_cas_per_s": n / (ph[0] / 1e3), "probes_per_s": n / (ph[3] / 1e3)}} if fam == "npo" else {}),
         "gpu_launches": kernels_per_step * args.steps,
         "clocks": clk.summary(),
         "result": {"count": total[0], "checksum": hex(total[1]), "over_ranks": world},
