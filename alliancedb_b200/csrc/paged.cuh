@@ -127,20 +127,22 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x, int lane) {
 // unit of a segment).  Per tile of up to kPTile tuples:
 //   A  every thread ranks its tuples within their digit (shared atomics on
 //      cnt[tile parity][d]);
-//   B  warps 0 .. F/32 - 1 (one digit per lane) turn the counts into the
-//      tile's digit runs (toff), take the pages each digit's stream needs from
-//      the CTA's pool, and advance the streams (npos = next free slot of the
-//      digit's current page, kNone when there is none);
+//   B  warp 0 (up to 128 digits, F / 32 per lane) or warps 0 .. F/32 - 1 (one
+//      digit per lane) turn the counts into the tile's digit runs (toff), take
+//      the pages each digit's stream needs from the CTA's pool, and advance
+//      the streams (npos = next free slot of the digit's current page, kNone
+//      when there is none);
 //   C  every thread puts its tuples into the stage, grouped by digit;
 //   D  every thread copies stage slots to their pages: slot i of digit d goes
 //      to i + b1[d] while i < lim[d] (the rest of the current page), else to
-//      i + b2[d] (the pages taken in B, consecutive in the pool).
+//      i + b2[d] (the pages taken in B, consecutive in the pool); the thread
+//      that writes a page's first slot also writes the page's log entry.
 // Consecutive stage slots of a digit go to consecutive addresses, so warps
 // store contiguous runs; a run's partial first and last 32-byte sectors are
 // completed by the neighbouring tiles of the same stream while the line is
-// still in L2.  Three barriers per tile (four above 32 digits); the next
-// tile's loads are in flight during D.  kMode: 0 flat input, 1 paged input (pass 2), 2 segmented flat
-// input (batched windows).
+// still in L2.  Three barriers per tile (four above 128 digits); the next
+// tile's loads are in flight during D.  kMode: 0 flat input, 1 paged input
+// (pass 2), 2 segmented flat input (batched windows).
 template <int kMode, int kThreads>
 __global__ void __launch_bounds__(kThreads, kPassMinBlocks)
 partition_pass(PassArgs a) {
