@@ -87,8 +87,8 @@ def test_radix_bits(oracle, algo, bits):
 
 @pytest.mark.parametrize("algo", ["PRO", "PRH"])
 @pytest.mark.parametrize("bits", [10, 13])
-def test_wide_pass_sizes(oracle, algo, bits):
-    """One-pass fan-outs of 2^10 .. 2^13 over several tiles per CTA, skewed S."""
+def test_two_pass_fanouts_many_tiles(oracle, algo, bits):
+    """Two-pass fan-outs (2^5 x 2^5, 2^6 x 2^7) over several tiles per CTA and pass-2 unit, skewed S."""
     R, S = fk_pair((1 << 21) + 5, (1 << 21) + 77, 1.0)
     check(oracle, algo, R, S, radix_bits=bits)
 
