@@ -45,7 +45,7 @@ class JoinParams(C.Structure):
         ("batch_tuples", C.c_int32),
         ("seed", C.c_uint64),
         ("realtime", C.c_int32),
-        ("reserved", C.c_int32),
+        ("test_flags", C.c_int32),
     ]
 
 

@@ -3,7 +3,9 @@
 libadb_b200.so   the CUDA join library (sm_100a only), from alliancedb_b200/csrc/*.cu
 liboracle.so     the CPU checker used by tests (oracle/adb_oracle.c), built beside it
 
-Run as ``python -m alliancedb_b200.build`` or through ``__graft_entry__.build()``.
+Run as ``python -m alliancedb_b200.build [AllianceDB source tree]`` (or with
+ADB_REF_ROOT set) or through ``__graft_entry__.build()``; without a source
+tree only the product library and the C restatement are built.
 Objects go to _build/ (not committed); the shared libraries stay in the tree
 so they travel with the repository snapshot.
 """
@@ -65,32 +67,39 @@ def build_cuda(verbose: bool = False) -> Path:
     return LIB
 
 
-REF_SRC = Path("/root/reference/hashing")
+def ref_root(explicit: str | None = None) -> Path | None:
+    """The AllianceDB source tree (its hashing/ and sorting/ directories), from
+    the argument or the ADB_REF_ROOT environment variable; None when neither
+    names an existing directory (the reference builds are then skipped)."""
+    r = explicit or os.environ.get("ADB_REF_ROOT")
+    return Path(r) if r and (Path(r) / "hashing").is_dir() else None
 
 
-def build_oracle() -> Path:
+def build_oracle(ref: Path | None = None) -> Path:
     """The CPU checker: the C restatement, and (when the AllianceDB sources are
-    present on this machine) the reference's own joins under oracle/_ref/."""
+    given) the reference's own joins under oracle/_ref/."""
     _run(["make", "-s", "-C", str(ROOT / "oracle"), "liboracle.so"])
-    if REF_SRC.is_dir():
-        _run(["make", "-s", "-C", str(ROOT / "oracle"), "ref", "read", f"REF_SRC={REF_SRC}"])
+    if ref is not None:
+        _run(["make", "-s", "-C", str(ROOT / "oracle"), "ref", "read", f"REF_SRC={ref / 'hashing'}"])
     return ORACLE_LIB
 
 
-def build_shim() -> None:
+def build_shim(ref: Path | None = None) -> None:
     """oracle/_ref/adb_ref_bench_gpu: the reference-side shim (its join
     signatures on libadb_b200.so) under the test harness; needs the
-    reference's headers, so only where its sources are present."""
-    if REF_SRC.is_dir():
-        _run(["make", "-s", "-C", str(ROOT / "oracle"), "shim", f"REF_SRC={REF_SRC}"])
+    reference's headers, so only where its sources are given."""
+    if ref is not None:
+        _run(["make", "-s", "-C", str(ROOT / "oracle"), "shim", f"REF_SRC={ref / 'hashing'}"])
 
 
-def build_all(verbose: bool = False) -> None:
-    build_oracle()
+def build_all(verbose: bool = False, ref: str | None = None) -> None:
+    r = ref_root(ref)
+    build_oracle(r)
     build_cuda(verbose)
-    build_shim()
+    build_shim(r)
 
 
 if __name__ == "__main__":
-    build_all(verbose="-v" in sys.argv)
+    args = [a for a in sys.argv[1:] if a != "-v"]
+    build_all(verbose="-v" in sys.argv, ref=args[0] if args else None)
     print(LIB)

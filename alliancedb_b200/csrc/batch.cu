@@ -289,6 +289,7 @@ int batch_launch(Context *ctx, const uint64_t *dR, const uint64_t *r_off, const 
     ja.chunk_off = chunk_off; ja.cstart = cstart;
     ja.n_items = ctr; ja.work_counter = ctr + 1;
     ja.acc = acc; ja.err = reinterpret_cast<int *>(acc + 2);
+    ja.waits_run_out = 0;
     ja.F = Dt;
     ja.bits = 0;   // per-window fan-out: the kernel reads each window's bits
     ja.mat = nullptr; ja.mat_n = nullptr; ja.mat_cap = 0;

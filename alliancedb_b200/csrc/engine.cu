@@ -343,6 +343,7 @@ int adb_join_device(const char *algo, const adb_tuple *dR, uint64_t nR, const ad
     s = ctx->ws.reserve(scratch_for(a, nR, nS, p, ctx->num_sms) + 4096);
     if (s == ADB_OK) {
         DevJoin j{reinterpret_cast<const uint64_t *>(dR), nR, reinterpret_cast<const uint64_t *>(dS), nS};
+        j.test_flags = p ? p->test_flags : 0;
         s = join_device_core(ctx, a, j, p, out, 0);
     }
     ctx->stream = saved;
@@ -373,6 +374,7 @@ int adb_join_materialize_device(const char *algo, const adb_tuple *dR, uint64_t 
     if (s == ADB_OK) {
         DevJoin j{reinterpret_cast<const uint64_t *>(dR), nR, reinterpret_cast<const uint64_t *>(dS), nS,
                   reinterpret_cast<uint64_t *>(dOut), cap};
+        j.test_flags = p ? p->test_flags : 0;
         s = join_device_core(ctx, a, j, p, out, 0);
     }
     ctx->stream = saved;
@@ -403,6 +405,7 @@ int adb_join(const char *algo, const adb_tuple *R, uint64_t nR, const adb_tuple 
     if (nS) ADB_CK(cudaMemcpyAsync(dS, S, nS * 8, cudaMemcpyHostToDevice, st));
     ADB_CK(cudaEventRecord(ctx->ev[5], st));
     DevJoin j{dR, nR, dS, nS};
+    j.test_flags = p ? p->test_flags : 0;
     s = join_device_core(ctx, a, j, p, out, ctx->ws.off);
     float th = 0;
     if (cudaEventElapsedTime(&th, ctx->ev[4], ctx->ev[5]) == cudaSuccess) out->ms_h2d = th;

@@ -16,6 +16,7 @@ struct DevJoin {
     uint64_t nS;
     uint64_t *mat = nullptr;      // optional <S-key, S-payload> output
     uint64_t mat_cap = 0;
+    int test_flags = 0;           // adb_join_params.test_flags
 };
 
 struct JoinTimes {

@@ -19,7 +19,9 @@
 // is only a stand-in symbol, not a device address.  The device address is
 // looked up once per device with cudaGetSymbolAddress, by the first call made
 // while that device is current, and cached.  Make that first call before any
-// stream capture.
+// stream capture.  The cached address belongs to the device's primary context:
+// after cudaDeviceReset (or anything else that destroys that context) the
+// library must be reloaded before this entry point is used again.
 //
 // Every call on a device shares the one array and leaves the last call's
 // contents behind; each call clears the table part it uses and the result
@@ -34,6 +36,11 @@ namespace adb {
 
 constexpr uint64_t kNoAllocTableSlots = 1ULL << 22;                 // 32 MiB of slots
 constexpr uint64_t kNoAllocMaxBuild = kNoAllocTableSlots / 2;       // 2^21 build tuples
+// A table of 2^ceil(log2(2 nR)) <= kNoAllocTableSlots slots is at most half
+// full, so every insert finds an empty slot before it has tried them all and
+// npo_build never sets its table-full error word: the two result words are the
+// whole outcome of a call.
+static_assert(2 * kNoAllocMaxBuild <= kNoAllocTableSlots, "the fixed table must stay at most half full");
 
 // [0, kNoAllocTableSlots) table slots, then count, checksum, error word,
 // sentinel counter.

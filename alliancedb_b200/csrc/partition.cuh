@@ -27,19 +27,6 @@ struct DigitFn {
     __host__ __device__ __forceinline__ uint32_t operator()(uint32_t key) const { return (key >> shift) & mask; }
 };
 
-struct RelPair {
-    const uint64_t *in[2];
-    uint64_t n[2];
-    uint64_t *out[2];
-};
-
-// Workspace layout of one partition call (all device pointers).
-struct PartWs {
-    uint32_t *hist;        // [2][F][G]  counts, then row-exclusive offsets
-    uint32_t *totals;      // [2][F]
-    uint64_t *starts;      // [2][F+1]  partition start offsets (exclusive scan), starts[F] = n
-};
-
 __host__ __device__ __forceinline__ uint64_t chunk_of(uint64_t n, int G) {
     uint64_t c = (n + G - 1) / G;
     return (c + 1) & ~1ULL;                     // even -> 16-byte aligned chunk starts

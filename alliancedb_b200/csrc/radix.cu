@@ -261,6 +261,7 @@ int run_radix(Context *ctx, const DevJoin &j, bool hist_table, int bits, unsigne
     a.chunk_off = chunk_off; a.cstart = cstart;
     a.n_items = ctr; a.work_counter = ctr + 1;
     a.acc = acc; a.err = reinterpret_cast<int *>(acc + 2);
+    a.waits_run_out = j.test_flags & ADB_TEST_WAITS_RUN_OUT;
     a.F = F; a.bits = (uint32_t)bits;
     a.mat = j.mat; a.mat_n = acc + 3; a.mat_cap = j.mat_cap;
     a.wbase = nullptr; a.wbits = nullptr; a.nwin = 0; a.wacc = nullptr;

@@ -253,6 +253,7 @@ struct JoinArgs {
     uint32_t *work_counter;
     unsigned long long *acc;         // [0] count, [1] checksum
     int *err;
+    int waits_run_out;               // ADB_TEST_WAITS_RUN_OUT: report completed waits as run out
     uint32_t F;
     uint32_t bits;                   // bits the partitioning consumed (the hash skips them)
     uint64_t *mat;                   // optional <S-key, S-payload> output
@@ -447,7 +448,7 @@ radix_join_items(JoinArgs a) {
         if (nb < 1) nb = 1;
         const uint32_t bmask = nb - 1;
         for (uint32_t i = threadIdx.x; i < nb + 2; i += blockDim.x) heads[i] = 0;
-        if (!mbar_wait(bar, phase)) atomicExch(a.err, 1);
+        if (!mbar_wait(bar, phase) || a.waits_run_out) atomicExch(a.err, 1);
         phase ^= 1;
         __syncthreads();
 

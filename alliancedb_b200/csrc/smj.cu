@@ -53,6 +53,7 @@ struct SmjArgs {
     uint32_t *work_counter;
     unsigned long long *acc;
     int *err;
+    int waits_run_out;               // ADB_TEST_WAITS_RUN_OUT: report completed waits as run out
     uint32_t F;
     uint64_t *mat;
     unsigned long long *mat_n;
@@ -193,7 +194,7 @@ smj_items(SmjArgs a) {
                          ((c + 1) & ~1u) * 8, bar);
             }
         }
-        if (!mbar_wait(bar, phase)) atomicExch(a.err, 1);
+        if (!mbar_wait(bar, phase) || a.waits_run_out) atomicExch(a.err, 1);
         phase ^= 1;
         __syncthreads();
         for (uint32_t k = threadIdx.x; k < np; k += blockDim.x) {
@@ -336,6 +337,7 @@ int run_smj(Context *ctx, const DevJoin &j, int part_fanout, bool /*multipass*/,
     a.pstart = po.pstart; a.items_off = items_off; a.chunk_off = chunk_off; a.cstart = cstart;
     a.n_items = ctr; a.work_counter = ctr + 1;
     a.acc = acc; a.err = reinterpret_cast<int *>(acc + 2);
+    a.waits_run_out = j.test_flags & ADB_TEST_WAITS_RUN_OUT;
     a.F = F;
     a.mat = j.mat; a.mat_n = acc + 3; a.mat_cap = j.mat_cap;
     smj_items<<<ctx->num_sms, kSmjThreads, kSmjSmem, st>>>(a);

@@ -47,11 +47,10 @@ ALG_BYTES = {"PRO": 24, "RJ_st": 24, "PRH": 24, "PRHO": 24, "NPO": 16, "NPO_st":
              "m-way": 24, "m-pass": 24, "m-way+skew": 24}
 # Per family: phase index (adb_join_result.ms_phase) -> (kernel, algorithmic
 # bytes per input tuple of one launch, DRAM bytes per input tuple of one launch
-# measured by ncu on |R| = |S| = 2^24 (profiles/partition_pass_pro_2e24.md,
-# profiles/radix_join_items_pro_2e24.md, profiles/smj_items_mway_2e24.md), None
-# where not captured).  The traffic of a full-size launch is that figure times
-# the launch's tuples: the kernels stream every tuple once, so traffic grows in
-# proportion.
+# from an ncu capture of dram__bytes_read.sum + dram__bytes_write.sum at
+# |R| = |S| = 2^24, None where not captured).  The traffic of a full-size
+# launch is that figure times the launch's tuples: the kernels stream every
+# tuple once, so traffic grows in proportion.
 KERNELS = {
     "radix": {0: ("partition_pass<0,512> (pass 1)", 16, (270285568 + 214802176) / 2**25),
               1: ("partition_pass<1,512> (pass 2)", 16, (273331456 + 214424576) / 2**25),
@@ -134,38 +133,57 @@ class ClockSampler:
         return out
 
 
-def load_traffic(kernel: str):
-    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
-    f = ROOT / "profiles" / "traffic.json"
-    if f.exists():
-        d = json.loads(f.read_text())
-        return d.get(kernel)
-    return None
-
-
 def make_inputs(adb, n: int, theta: float, seed: int):
     R = adb.gen_pk(n, seed)
-    S = adb.gen_fk(n, R, theta, seed + 1)
-    return R, S
+    S, idx = adb.gen_fk(n, R, theta, seed + 1, want_idx=True)
+    return R, S, idx
 
 
-def cpu_baseline_port(algo: str, n_sample: int, budget_s: float):
-    """Time the oracle's CPU restatement (single thread) on samples of the workload."""
-    import alliancedb_b200 as adb
+def _fmix64(z):
+    z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def fk_closed_form(R, S, idx):
+    """(count, checksum) of a foreign-key join from the generator's drawn
+    indices: S tuple j matches R tuple idx[j] and nothing else (R's keys are
+    unique), so count = |S| and checksum = sum_j H(R.key[idx_j], R.payload[idx_j],
+    S.payload[j]) mod 2^64, H the pair hash of the result contract.  numpy,
+    chunked over host threads; runs outside every timed region."""
+    import concurrent.futures as cf
+    Rw, Sw = R.view(np.uint64), S.view(np.uint64)
+    lo = np.uint64(0xFFFFFFFF)
+    s32 = np.uint64(32)
+
+    def part(b):
+        e = min(len(Sw), b + (1 << 22))
+        rw = Rw[idx[b:e]]
+        key, rp = rw >> s32, rw & lo
+        sp = Sw[b:e] & lo
+        h = _fmix64(((key << s32) | rp) ^ _fmix64((sp << s32) | key))
+        return int(h.sum(dtype=np.uint64))
+
+    with cf.ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 1)) as ex:
+        total = sum(ex.map(part, range(0, len(Sw), 1 << 22)))
+    return len(Sw), total % (1 << 64)
+
+
+def cpu_baseline_port(algo: str, R, S, budget_s: float):
+    """Time the oracle's CPU restatement (single thread) on the workload: calls
+    until budget_s seconds have run (at least one); returns (tuples/s, calls)."""
     from tests.oracle_bind import Oracle
     o = Oracle()
     fn = {"PRO": o.pro, "RJ_st": o.pro, "PRH": o.prh, "PRHO": o.prh, "NPO": o.npo, "NPO_st": o.npo,
           "m-way": o.smj, "m-pass": o.smj, "m-way+skew": o.smj}[algo]
-    R, S = make_inputs(adb, n_sample, 0.0, 101)
-    done, t_tot, reps = 0, 0.0, 0
+    t_tot, reps = 0.0, 0
     while t_tot < budget_s or reps < 1:
         t0 = time.perf_counter()
         cnt, _ = fn(R, S)
         t_tot += time.perf_counter() - t0
-        assert cnt == n_sample
-        done += 2 * n_sample
+        assert cnt == len(S)
         reps += 1
-    return done / t_tot, reps
+    return (len(R) + len(S)) * reps / t_tot, reps
 
 
 REF_ALGOS = ("PRO", "PRH", "RJ_st", "NPO", "NPO_st")
@@ -178,40 +196,47 @@ def host_threads():
         return os.cpu_count() or 1
 
 
-def ref_cpu(algo: str, n_sample: int, threads: int, reps: int):
+def ref_cpu(algo: str, n: int, theta: float, threads: int, reps: int, warmup: int, budget_s: float):
     """The reference's own join (oracle/_ref, compiled from its sources) on this
-    host: median tuples/s over `reps` calls after one warm-up, or None when the
-    reference build is absent or lacks `algo`."""
+    host, on the benchmark's relations (n tuples per side, S Zipf(theta) over R's
+    keys): `warmup` untimed calls, then up to `reps` timed calls, stopping once
+    budget_s seconds of timed calls have run.  Returns the harness's JSON
+    (median ms, tuples_per_s, reps made), or None when the reference build is
+    absent or lacks `algo`."""
     ref = ROOT / "oracle" / "_ref" / "adb_ref_bench"
     if not ref.exists() or algo not in REF_ALGOS:
         return None
-    out = subprocess.run([str(ref), algo, "gen", str(n_sample), str(threads), str(max(1, reps))], check=True,
-                         capture_output=True, text=True, timeout=600).stdout
+    out = subprocess.run([str(ref), algo, "gen", str(n), str(threads), str(max(1, reps)), str(theta),
+                          str(warmup), str(budget_s)], check=True, capture_output=True, text=True,
+                         timeout=1800).stdout
     d = json.loads(out.strip().splitlines()[-1])
-    if d["count"] != n_sample:
-        raise RuntimeError(f"reference join returned {d['count']} matches, expected {n_sample}")
-    return d["tuples_per_s"]
+    if d["count"] != n:
+        raise RuntimeError(f"reference join returned {d['count']} matches, expected {n}")
+    return d
 
 
 def reference_arm(args):
-    """--impl reference: the reference's CPU join on this host (rank 0 only)."""
+    """--impl reference: the reference's CPU join on this host (rank 0 only),
+    on the full workload of `config` (same n and theta as our arm)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    n_sample = 1 << min(args.log2n, 24)
+    n = 1 << args.log2n
     threads = host_threads()
-    value = ref_cpu(args.algo, n_sample, threads, args.steps)
-    if value is not None:
-        kind, cores = "reference", threads
-        sample = (f"{args.algo} |R|=|S|=2^{n_sample.bit_length() - 1} PK-FK, reference code compiled from its "
-                  f"sources, {threads} threads, median of {args.steps} join calls after 1 warm-up")
+    warm = min(args.warmup, 2)
+    d = ref_cpu(args.algo, n, args.theta, threads, args.steps, warm, args.ref_budget)
+    if d is not None:
+        value, kind, cores = d["tuples_per_s"], "reference", threads
+        sample = (f"{args.algo} |R|=|S|=2^{args.log2n}, S Zipf theta={args.theta} over R's keys (the full "
+                  f"workload), reference code compiled from its sources, {threads} threads, median of "
+                  f"{d['reps']} timed join calls after {warm} warm-up calls, fresh input copies per call")
     else:
-        vals = []
-        for _ in range(args.steps):
-            v, _ = cpu_baseline_port(args.algo, min(n_sample, 1 << 22), 2.0)
-            vals.append(v)
-        value, kind, cores = statistics.median(vals), "port", 1
-        sample = f"{args.algo} |R|=|S|=2^{min(args.log2n, 22)} PK-FK, oracle restatement, 1 thread"
+        import alliancedb_b200 as adb
+        R, S, _ = make_inputs(adb, n, args.theta, 1)
+        value, reps = cpu_baseline_port(args.algo, R, S, args.ref_budget)
+        kind, cores = "port", 1
+        sample = (f"{args.algo} |R|=|S|=2^{args.log2n}, S Zipf theta={args.theta} (the full workload), "
+                  f"oracle restatement, 1 thread, {reps} calls")
     line = {"impl": "reference", "metric": "join input tuples/s", "value": value, "unit": "tuples/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32 key/payload (integer)", "data": "synthetic",
@@ -238,7 +263,10 @@ def main():
     ap.add_argument("--algo", default="PRO")
     ap.add_argument("--log2n", type=int, default=27)
     ap.add_argument("--theta", type=float, default=0.0)
-    ap.add_argument("--cpu-budget", type=float, default=10.0)
+    ap.add_argument("--cpu-budget", type=float, default=20.0,
+                    help="seconds of timed reference calls for the cpu_baseline of our arm")
+    ap.add_argument("--ref-budget", type=float, default=120.0,
+                    help="--impl reference: stop timing once this many seconds of calls have run")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="join", choices=["join", "batch", "serve", "stream"],
                     help="join: one R/S pair (default, the headline); batch: 4096 windows, one launch "
@@ -275,7 +303,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     n = 1 << args.log2n
-    R, S = make_inputs(adb, n, args.theta, 1 + 1000 * rank)
+    R, S, idx = make_inputs(adb, n, args.theta, 1 + 1000 * rank)
     dev = torch.device("cuda", local)
     dR = torch.from_numpy(R.view(np.int64)).to(dev)
     dS = torch.from_numpy(S.view(np.int64)).to(dev)
@@ -296,8 +324,12 @@ def main():
 
     for _ in range(args.warmup):
         r = step()
-    assert r.count == n, f"FK join must match every S tuple once: {r.count} != {n}"
     want = (r.count, r.checksum)
+    # the result against the closed form of the foreign-key workload (untimed)
+    closed = fk_closed_form(R, S, idx)
+    if want != closed:
+        raise AssertionError(f"join result {want[0]}, {want[1]:#x} != closed form {closed[0]}, {closed[1]:#x}")
+    del idx
 
     # ---- device-resident timed region
     phases = []
@@ -377,19 +409,24 @@ def main():
             "build_cas_per_s": n / (ph[0] / 1e3), "probes_per_s": n / (ph[3] / 1e3)}} if fam == "npo" else {}),
         "gpu_launches": kernels_per_step * args.steps,
         "clocks": clk.summary(),
-        "result": {"count": total[0], "checksum": hex(total[1]), "over_ranks": world},
+        "result": {"count": total[0], "checksum": hex(total[1]), "over_ranks": world,
+                   "verified": "equal to the closed form of the foreign-key workload on every rank (numpy, "
+                               "from the generator's drawn indices)"},
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = host_threads()
-        v = ref_cpu(args.algo, 1 << 24, threads, 5)
-        if v is not None:
-            line["cpu_baseline"] = {"value": v, "unit": "tuples/s", "cores": threads, "kind": "reference",
-                                    "sample": f"reference {args.algo} on |R|=|S|=2^24 PK-FK, {threads} threads, "
-                                              "median of 5 join calls"}
+        d = ref_cpu(args.algo, n, args.theta, threads, 3, 1, args.cpu_budget)
+        if d is not None:
+            line["cpu_baseline"] = {"value": d["tuples_per_s"], "unit": "tuples/s", "cores": threads,
+                                    "kind": "reference",
+                                    "sample": f"reference {args.algo} on the full workload (|R|=|S|=2^{args.log2n}, "
+                                              f"theta={args.theta}), {threads} threads, median of {d['reps']} "
+                                              "timed join calls after 1 warm-up"}
         else:
-            v, reps = cpu_baseline_port(args.algo, 1 << 22, args.cpu_budget)
+            v, reps = cpu_baseline_port(args.algo, R, S, args.cpu_budget)
             line["cpu_baseline"] = {"value": v, "unit": "tuples/s", "cores": 1, "kind": "port",
-                                    "sample": f"oracle {args.algo} restatement on |R|=|S|=2^22 FK, {reps} runs"}
+                                    "sample": f"oracle {args.algo} restatement on the full workload "
+                                              f"(|R|=|S|=2^{args.log2n}, theta={args.theta}), {reps} calls"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -82,8 +82,13 @@ typedef struct adb_join_params {
     uint64_t seed;              /* JBCR's random split of S */
     int32_t realtime;           /* adb_stream_join: 1 = release each micro-batch at its timestamp
                                    (wall clock, the reference's WAIT gating, fetcher.cpp:120-190) */
-    int32_t reserved;
+    int32_t test_flags;         /* 0 in normal use.  ADB_TEST_WAITS_RUN_OUT: every bounded device wait
+                                   of the partitioned and sort-merge joins, once it has completed,
+                                   reports that it ran out, so callers can test their ADB_ERR_TIMEOUT
+                                   handling without making a GPU wait for real */
 } adb_join_params;
+
+#define ADB_TEST_WAITS_RUN_OUT 1
 
 typedef struct adb_join_result {
     uint64_t count;             /* result_t.totalresults */
@@ -271,7 +276,8 @@ int adb_release_workspace(void);
  * count, checksum.  Runs on `stream` (a cudaStream_t, NULL = the default
  * stream) and returns without synchronising.  The first call on each device
  * looks up the array's device address (cudaGetSymbolAddress) and caches it;
- * make that first call before any stream capture.  All calls on a device
+ * make that first call before any stream capture.  The cached address does not
+ * survive cudaDeviceReset: reload the library after a reset.  All calls on a device
  * share the one array: calls that overlap on the GPU race and must be
  * serialised by the caller. */
 int adb_npo_join_noalloc(const adb_tuple *dR, uint64_t nR, const adb_tuple *dS, uint64_t nS,

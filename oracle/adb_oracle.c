@@ -446,3 +446,45 @@ uint64_t ora_materialize_sorted(const ora_tuple *R, uint64_t nR, const ora_tuple
     free(r); free(s);
     return n;
 }
+
+/* ------------------------------------------------------------------ */
+/* Direct-address truth for a build side with unique keys (the PK side */
+/* of every foreign-key configuration).  payload_of[key] and a         */
+/* presence bit per key are filled from R, then each S tuple looks up  */
+/* its key: no partitioning, hashing or sorting, so it shares nothing  */
+/* with the restatements above and stays cheap at 2^27 tuples.         */
+/* ------------------------------------------------------------------ */
+int ora_pk_truth(const ora_tuple *R, uint64_t nR, const ora_tuple *S, uint64_t nS, ora_result *out) {
+    out->count = 0;
+    out->checksum = 0;
+    uint64_t maxkey = 0;
+    for (uint64_t i = 0; i < nR; i++)
+        if (R[i].key > maxkey) maxkey = R[i].key;
+    if (maxkey > 8 * nR + (1u << 20)) return -2;   /* keys not dense enough for a direct table */
+    const uint64_t slots = maxkey + 1;
+    uint32_t *payload_of = (uint32_t *)malloc(sizeof(uint32_t) * slots);
+    uint64_t *present = (uint64_t *)calloc((slots + 63) / 64, sizeof(uint64_t));
+    if (!payload_of || !present) { free(payload_of); free(present); return -3; }
+    for (uint64_t i = 0; i < nR; i++) {
+        if (i + 16 < nR && R[i + 16].key <= maxkey) {
+            __builtin_prefetch(&payload_of[R[i + 16].key], 1);
+            __builtin_prefetch(&present[R[i + 16].key >> 6], 1);
+        }
+        const uint32_t k = R[i].key;
+        const uint64_t bit = 1ull << (k & 63);
+        if (present[k >> 6] & bit) { free(payload_of); free(present); return -1; }   /* repeated key */
+        present[k >> 6] |= bit;
+        payload_of[k] = R[i].payload;
+    }
+    for (uint64_t j = 0; j < nS; j++) {
+        if (j + 16 < nS && S[j + 16].key <= maxkey) {   /* random lookups: keep several in flight */
+            __builtin_prefetch(&payload_of[S[j + 16].key]);
+            __builtin_prefetch(&present[S[j + 16].key >> 6]);
+        }
+        const uint32_t k = S[j].key;
+        if (k <= maxkey && (present[k >> 6] >> (k & 63)) & 1) emit(out, k, payload_of[k], S[j].payload);
+    }
+    free(payload_of);
+    free(present);
+    return 0;
+}

@@ -46,6 +46,11 @@ int ora_pmj(const ora_tuple *R, uint64_t nR, const ora_tuple *S, uint64_t nS,
 /* Independent truth: sort both by key, multiply run lengths, enumerate pairs. */
 int ora_truth(const ora_tuple *R, uint64_t nR, const ora_tuple *S, uint64_t nS, ora_result *out);
 
+/* Truth for R with unique keys by direct addressing on the key (no
+ * partitioning, hashing or sorting).  Returns -1 when R repeats a key, -2 when
+ * R's largest key exceeds 8 |R| + 2^20 (no direct table), -3 out of memory. */
+int ora_pk_truth(const ora_tuple *R, uint64_t nR, const ora_tuple *S, uint64_t nS, ora_result *out);
+
 /* Result materialisation: writes <S-key, S-payload> per match (the reference's
  * JOIN_RESULT_MATERIALIZE output), sorted as 64-bit words; returns the count. */
 uint64_t ora_materialize_sorted(const ora_tuple *R, uint64_t nR, const ora_tuple *S, uint64_t nS,

@@ -4,13 +4,20 @@
 // (bench.py --impl reference) timed on the host's cores.
 //
 // Usage:
-//   adb_ref_bench <PRO|PRH|RJ_st|NPO|NPO_st> gen <n> <threads> <reps>
+//   adb_ref_bench <PRO|PRH|RJ_st|NPO|NPO_st> gen <n> <threads> <reps> [theta] [warmup] [budget_s]
 //       PK-FK relations of n tuples each (R keys a seeded permutation of 1..n,
-//       S keys drawn uniformly from R's keys; the generator of the benchmark
-//       configs, restated here), one warm-up call, then reps timed calls
+//       S keys drawn from R's keys uniformly (theta 0) or Zipf(theta) through a
+//       seeded rank permutation; the generator of the benchmark configs,
+//       restated here), `warmup` untimed calls (default 1 when reps > 1), then
+//       up to reps timed calls, stopping early once budget_s seconds of timed
+//       calls have run (at least one timed call)
 //   adb_ref_bench <algo> files <R.bin> <S.bin> <threads>
 //       relations from files of 8-byte {payload, key} tuples, one call
-// Prints one JSON line: algo, n_r, n_s, threads, count, ms (median), tuples_per_s.
+//   adb_ref_bench dump <n> <theta> <R.bin> <S.bin>
+//       writes the relations that `gen` would join (to check the restated
+//       generator against the benchmark's)
+// Prints one JSON line: algo, n_r, n_s, threads, count, ms (median), reps (timed
+// calls made), tuples_per_s.
 //
 // Built twice by oracle/Makefile: adb_ref_bench links the reference's join
 // objects; adb_ref_bench_gpu (ADB_SHIM defined) links the same calls against
@@ -25,6 +32,8 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
+#include <thread>
 #include <cstring>
 #include <fstream>
 #include <string>
@@ -92,19 +101,73 @@ static tuple_t *alloc_rel(uint64_t n) {
     return (tuple_t *)alloc_aligned(n * sizeof(tuple_t) + RELATION_PADDING);
 }
 
-static void gen_pkfk(uint64_t n, std::vector<tuple_t> &R, std::vector<tuple_t> &S) {
+// Zipf(theta) rank in [0, n) by rejection-inversion (Hormann and Derflinger,
+// ACM TOMACS 6(3), 1996), as the benchmark generator draws it.
+struct ZipfRank {
+    double s, n, hx1, hn, sq;
+    static double helper1(double x) { return fabs(x) > 1e-8 ? log1p(x) / x : 1.0 - x * (0.5 - x * (1.0 / 3.0 - 0.25 * x)); }
+    static double helper2(double x) {
+        return fabs(x) > 1e-8 ? expm1(x) / x : 1.0 + x * 0.5 * (1.0 + x * (1.0 / 3.0) * (1.0 + 0.25 * x));
+    }
+    double h(double x) const { return exp(-s * log(x)); }
+    double hint(double x) const {
+        const double lx = log(x);
+        return helper2((1.0 - s) * lx) * lx;
+    }
+    double hinv(double x) const {
+        double t = x * (1.0 - s);
+        if (t < -1.0) t = -1.0;
+        return exp(helper1(t) * x);
+    }
+    ZipfRank(uint64_t n_, double theta) : s(theta), n((double)n_) {
+        hx1 = hint(1.5) - 1.0;
+        hn = hint(n + 0.5);
+        sq = 2.0 - hinv(hint(2.5) - h(2.0));
+    }
+    uint64_t sample(uint64_t seed, uint64_t j) const {
+        for (uint32_t attempt = 0; attempt < 64; attempt++) {
+            const double u01 = ((mix3(seed, 7, j * 64 + attempt) >> 11) + 1) * (1.0 / 9007199254740992.0);
+            const double u = hn + u01 * (hx1 - hn);
+            const double x = hinv(u);
+            double kd = floor(x + 0.5);
+            if (kd < 1.0) kd = 1.0;
+            if (kd > n) kd = n;
+            if (kd - x <= sq || u >= hint(kd + 0.5) - h(kd)) return (uint64_t)kd - 1;
+        }
+        return 0;
+    }
+};
+
+template <class F>
+static void par_for(uint64_t n, F f) {
+    unsigned nt = std::thread::hardware_concurrency();
+    if (nt == 0 || n < (1u << 16)) nt = 1;
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nt; t++) {
+        const uint64_t b = n * t / nt, e = n * (t + 1) / nt;
+        th.emplace_back([=] { for (uint64_t i = b; i < e; i++) f(i); });
+    }
+    for (auto &x : th) x.join();
+}
+
+// R: key = 1 + perm_1(i), payload = i.  S: payload = j, key = R.key[idx_j], idx_j
+// uniform over 0..n-1 (theta 0) or rank_perm(Zipf(theta) rank) (seed 2).
+static void gen_pkfk(uint64_t n, double theta, std::vector<tuple_t> &R, std::vector<tuple_t> &S) {
     R.resize(n);
     S.resize(n);
     Feistel perm(n ? n : 1, 1);
-    for (uint64_t i = 0; i < n; i++) {
+    par_for(n, [&](uint64_t i) {
         R[i].payloadID = (int32_t)i;
         R[i].key = (int32_t)(1 + perm(i));
-    }
-    for (uint64_t j = 0; j < n; j++) {
-        const uint64_t idx = (uint64_t)(((unsigned __int128)mix3(2, 3, j) * n) >> 64);
+    });
+    Feistel rank_perm(n ? n : 1, 2 ^ 0x5A5A5A5A5A5A5A5AULL);
+    ZipfRank z(n ? n : 1, theta > 0 ? theta : 1.0);
+    par_for(n, [&](uint64_t j) {
+        const uint64_t idx = theta > 0 ? rank_perm(z.sample(2, j))
+                                       : (uint64_t)(((unsigned __int128)mix3(2, 3, j) * n) >> 64);
         S[j].payloadID = (int32_t)j;
         S[j].key = R[idx].key;
-    }
+    });
 }
 
 static bool read_rel(const char *path, std::vector<tuple_t> &out) {
@@ -147,17 +210,32 @@ int main(int argc, char **argv) {
         return 2;
     }
     const std::string algo = argv[1];
+    if (algo == "dump" && argc >= 6) {
+        std::vector<tuple_t> R, S;
+        gen_pkfk(strtoull(argv[2], nullptr, 10), atof(argv[3]), R, S);
+        FILE *fr = fopen(argv[4], "wb"), *fs = fopen(argv[5], "wb");
+        if (!fr || !fs) return 2;
+        const bool ok = fwrite(R.data(), sizeof(tuple_t), R.size(), fr) == R.size() &&
+                        fwrite(S.data(), sizeof(tuple_t), S.size(), fs) == S.size();
+        fclose(fr);
+        fclose(fs);
+        return ok ? 0 : 1;
+    }
     join_fn fn = lookup(algo);
     if (!fn) {
         fprintf(stderr, "unsupported algorithm %s\n", algo.c_str());
         return 2;
     }
     std::vector<tuple_t> R0, S0;
-    int reps = 1;
+    int reps = 1, warmup = 0;
+    double budget_s = 1e30;
     if (std::string(argv[2]) == "gen" && argc >= 6) {
-        gen_pkfk(strtoull(argv[3], nullptr, 10), R0, S0);
+        const double theta = argc >= 7 ? atof(argv[6]) : 0.0;
+        gen_pkfk(strtoull(argv[3], nullptr, 10), theta, R0, S0);
         nthreads = atoi(argv[4]);
-        reps = atoi(argv[5]);
+        reps = std::max(1, atoi(argv[5]));
+        warmup = argc >= 8 ? std::max(0, atoi(argv[7])) : (reps > 1 ? 1 : 0);
+        if (argc >= 9) budget_s = atof(argv[8]);
     } else if (std::string(argv[2]) == "files" && argc >= 6) {
         if (!read_rel(argv[3], R0) || !read_rel(argv[4], S0)) {
             fprintf(stderr, "cannot read relations\n");
@@ -178,7 +256,8 @@ int main(int argc, char **argv) {
     std::vector<double> ms;
     int64_t count = -1;
     uint64_t checksum = 0;
-    for (int r = 0; r < reps + (reps > 1 ? 1 : 0); r++) {
+    double timed_s = 0;
+    for (int r = 0; r < warmup + reps; r++) {
         // fresh copies: PRO overwrites its inputs (parallel_radix_join.cpp:1176-1181)
         memcpy(rt, R0.data(), R0.size() * sizeof(tuple_t));
         memcpy(st, S0.data(), S0.size() * sizeof(tuple_t));
@@ -195,14 +274,17 @@ int main(int argc, char **argv) {
         checksum = adb_shim_checksum(res);
 #endif
         free(res);
-        if (reps > 1 && r == 0) continue;   // warm-up
+        if (r < warmup) continue;
         ms.push_back(std::chrono::duration<double, std::milli>(t1 - t0).count());
+        timed_s += ms.back() / 1e3;
+        if (timed_s >= budget_s) break;
     }
     std::sort(ms.begin(), ms.end());
     const double med = ms[ms.size() / 2];
     printf("{\"algo\": \"%s\", \"n_r\": %zu, \"n_s\": %zu, \"threads\": %d, \"count\": %lld, "
-           "\"checksum\": %llu, \"ms\": %.3f, \"tuples_per_s\": %.1f}\n",
+           "\"checksum\": %llu, \"ms\": %.3f, \"reps\": %zu, \"tuples_per_s\": %.1f}\n",
            algo.c_str(), R0.size(), S0.size(), nthreads, (long long)count, (unsigned long long)checksum, med,
+           ms.size(),
            (R0.size() + S0.size()) / (med / 1e3));
     return 0;
 }

@@ -43,11 +43,12 @@ class Oracle:
         L.ora_shj.argtypes = [P, U, P, U, R]
         L.ora_pmj.argtypes = [P, U, P, U, U, U, R]
         L.ora_truth.argtypes = [P, U, P, U, R]
+        L.ora_pk_truth.argtypes = [P, U, P, U, R]
         L.ora_materialize_sorted.argtypes = [P, U, P, U, P, U]
         L.ora_materialize_sorted.restype = U
         L.ora_pair_hash.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32]
         L.ora_pair_hash.restype = U
-        for f in ("ora_pro", "ora_prh", "ora_npo", "ora_smj", "ora_shj", "ora_pmj", "ora_truth"):
+        for f in ("ora_pro", "ora_prh", "ora_npo", "ora_smj", "ora_shj", "ora_pmj", "ora_truth", "ora_pk_truth"):
             getattr(L, f).restype = C.c_int
         self.L = L
 
@@ -79,6 +80,17 @@ class Oracle:
 
     def truth(self, R, S):
         return self._call(self.L.ora_truth, R, S)
+
+    def pk_truth(self, R, S):
+        """Truth for an R with unique keys, by direct addressing on the key
+        (linear time; used at the benchmark's full sizes)."""
+        Rw, Sw = _words(R), _words(S)
+        r = _Res()
+        st = self.L.ora_pk_truth(Rw.ctypes.data if Rw.size else None, Rw.size,
+                                 Sw.ctypes.data if Sw.size else None, Sw.size, C.byref(r))
+        if st != 0:
+            raise ValueError(f"ora_pk_truth: R's keys repeat or are not dense (status {st})")
+        return int(r.count), int(r.checksum)
 
     def pair_hash(self, key, rp, sp):
         return int(self.L.ora_pair_hash(key, rp, sp))

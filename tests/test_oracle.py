@@ -90,6 +90,25 @@ def test_pkfk_known_answer(oracle, theta):
     assert ck == int(closed)
 
 
+@pytest.mark.parametrize("theta", [0.0, 1.5])
+def test_pk_truth_equals_truth_and_closed_form(oracle, theta):
+    n = 1 << 16
+    R = adb.gen_pk(n, 21)
+    S, idx = adb.gen_fk(n + 77, R, theta, 22, want_idx=True)
+    got = oracle.pk_truth(R, S)
+    assert got == oracle.truth(R, S)
+    closed = pair_hash_np(R["key"][idx], R["payload"][idx], S["payload"]).sum(dtype=np.uint64)
+    assert got == (n + 77, int(closed))
+    # S keys absent from R do not match; R keys repeated are refused
+    S2 = S.copy()
+    S2["key"][:100] = n + 5
+    assert oracle.pk_truth(R, S2) == oracle.truth(R, S2)
+    R2 = R.copy()
+    R2["key"][1] = R2["key"][0]
+    with pytest.raises(ValueError):
+        oracle.pk_truth(R2, S)
+
+
 @pytest.mark.parametrize("n", [0, 1, 5])
 def test_oracle_tiny_and_empty(oracle, n):
     R = rnd(n, 3, 1)
@@ -117,3 +136,17 @@ def test_reference_binary_counts(oracle, tmp_path, algo):
     out = subprocess.run([str(REF_BIN), algo, "files", str(tmp_path / "R.bin"), str(tmp_path / "S.bin"), "4"],
                          capture_output=True, text=True, timeout=120, check=True).stdout
     assert json.loads(out.strip().splitlines()[-1])["count"] == oracle.truth(R, S)[0]
+
+
+@pytest.mark.skipif(not REF_BIN.exists(), reason="the reference binary is built only where its sources are")
+@pytest.mark.parametrize("theta", [0.0, 0.5, 1.5])
+def test_reference_harness_generator_is_the_benchmarks(tmp_path, theta):
+    """The reference arm of bench.py joins what the harness generates; it must be
+    the same relations as adb.gen_pk(n, 1) / adb.gen_fk(n, R, theta, 2)."""
+    n = 50000
+    subprocess.run([str(REF_BIN), "dump", str(n), str(theta), str(tmp_path / "R.bin"), str(tmp_path / "S.bin")],
+                   check=True, timeout=120)
+    R = adb.gen_pk(n, 1)
+    S = adb.gen_fk(n, R, theta, 2)
+    assert np.array_equal(np.fromfile(tmp_path / "R.bin", dtype=np.uint64), R.view(np.uint64))
+    assert np.array_equal(np.fromfile(tmp_path / "S.bin", dtype=np.uint64), S.view(np.uint64))
