@@ -80,7 +80,7 @@ def build_oracle(ref: Path | None = None) -> Path:
     given) the reference's own joins under oracle/_ref/."""
     _run(["make", "-s", "-C", str(ROOT / "oracle"), "liboracle.so"])
     if ref is not None:
-        _run(["make", "-s", "-C", str(ROOT / "oracle"), "ref", "read", f"REF_SRC={ref / 'hashing'}"])
+        _run(["make", "-s", "-j8", "-C", str(ROOT / "oracle"), "ref", "read", "ck", f"REF_ROOT={ref}"])
     return ORACLE_LIB
 
 
@@ -89,7 +89,7 @@ def build_shim(ref: Path | None = None) -> None:
     signatures on libadb_b200.so) under the test harness; needs the
     reference's headers, so only where its sources are given."""
     if ref is not None:
-        _run(["make", "-s", "-C", str(ROOT / "oracle"), "shim", f"REF_SRC={ref / 'hashing'}"])
+        _run(["make", "-s", "-C", str(ROOT / "oracle"), "shim", "shim-sort", f"REF_ROOT={ref}"])
 
 
 def build_all(verbose: bool = False, ref: str | None = None) -> None:

@@ -186,7 +186,8 @@ def cpu_baseline_port(algo: str, R, S, budget_s: float):
     return (len(R) + len(S)) * reps / t_tot, reps
 
 
-REF_ALGOS = ("PRO", "PRH", "RJ_st", "NPO", "NPO_st")
+REF_HASH_ALGOS = ("PRO", "PRH", "RJ_st", "NPO", "NPO_st")
+REF_SORT_ALGOS = ("m-way", "m-pass", "m-way+skew")
 
 
 def host_threads():
@@ -200,19 +201,23 @@ def ref_cpu(algo: str, n: int, theta: float, threads: int, reps: int, warmup: in
     """The reference's own join (oracle/_ref, compiled from its sources) on this
     host, on the benchmark's relations (n tuples per side, S Zipf(theta) over R's
     keys): `warmup` untimed calls, then up to `reps` timed calls, stopping once
-    budget_s seconds of timed calls have run.  Returns the harness's JSON
-    (median ms, tuples_per_s, reps made), or None when the reference build is
-    absent or lacks `algo`."""
-    ref = ROOT / "oracle" / "_ref" / "adb_ref_bench"
-    if not ref.exists() or algo not in REF_ALGOS:
+    budget_s seconds of timed calls have run.  The sort-merge joins run on the
+    largest power of two <= threads (sortmergejoin_multiway.cpp:59).  Returns
+    the harness's JSON (median ms, tuples_per_s, reps made, threads, count),
+    or None when the reference build is absent or lacks `algo`."""
+    if algo in REF_HASH_ALGOS:
+        ref = ROOT / "oracle" / "_ref" / "adb_ref_bench"
+    elif algo in REF_SORT_ALGOS:
+        ref = ROOT / "oracle" / "_ref" / "adb_ref_sort"
+        threads = 1 << (max(1, threads).bit_length() - 1)
+    else:
+        return None
+    if not ref.exists():
         return None
     out = subprocess.run([str(ref), algo, "gen", str(n), str(threads), str(max(1, reps)), str(theta),
                           str(warmup), str(budget_s)], check=True, capture_output=True, text=True,
                          timeout=1800).stdout
-    d = json.loads(out.strip().splitlines()[-1])
-    if d["count"] != n:
-        raise RuntimeError(f"reference join returned {d['count']} matches, expected {n}")
-    return d
+    return json.loads([ln for ln in out.splitlines() if ln.startswith("{")][-1])
 
 
 def reference_arm(args):
@@ -226,10 +231,11 @@ def reference_arm(args):
     warm = min(args.warmup, 2)
     d = ref_cpu(args.algo, n, args.theta, threads, args.steps, warm, args.ref_budget)
     if d is not None:
-        value, kind, cores = d["tuples_per_s"], "reference", threads
+        value, kind, cores = d["tuples_per_s"], "reference", d["threads"]
         sample = (f"{args.algo} |R|=|S|=2^{args.log2n}, S Zipf theta={args.theta} over R's keys (the full "
-                  f"workload), reference code compiled from its sources, {threads} threads, median of "
-                  f"{d['reps']} timed join calls after {warm} warm-up calls, fresh input copies per call")
+                  f"workload), reference code compiled from its sources, {d['threads']} threads, median of "
+                  f"{d['reps']} timed join calls after {warm} warm-up calls, fresh input copies per call; "
+                  f"the reference returned {d['count']} matches (|S| = {n})")
     else:
         import alliancedb_b200 as adb
         R, S, _ = make_inputs(adb, n, args.theta, 1)
@@ -417,11 +423,11 @@ def main():
         threads = host_threads()
         d = ref_cpu(args.algo, n, args.theta, threads, 3, 1, args.cpu_budget)
         if d is not None:
-            line["cpu_baseline"] = {"value": d["tuples_per_s"], "unit": "tuples/s", "cores": threads,
+            line["cpu_baseline"] = {"value": d["tuples_per_s"], "unit": "tuples/s", "cores": d["threads"],
                                     "kind": "reference",
                                     "sample": f"reference {args.algo} on the full workload (|R|=|S|=2^{args.log2n}, "
-                                              f"theta={args.theta}), {threads} threads, median of {d['reps']} "
-                                              "timed join calls after 1 warm-up"}
+                                              f"theta={args.theta}), {d['threads']} threads, median of {d['reps']} "
+                                              f"timed join calls after 1 warm-up; {d['count']} matches"}
         else:
             v, reps = cpu_baseline_port(args.algo, R, S, args.cpu_budget)
             line["cpu_baseline"] = {"value": v, "unit": "tuples/s", "cores": 1, "kind": "port",

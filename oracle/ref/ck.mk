@@ -1,0 +1,52 @@
+# TEST INFRASTRUCTURE ONLY -- included by oracle/Makefile once ref/ref_tree.py
+# has prepared the reference tree in _ref/src.  Builds, from that tree:
+#   _ref/adb_ref_ck_hash   hashing/ joins (PRO ... PMJ_*) with the checksum at the match sites
+#   _ref/adb_ref_ck_sort   sorting/ joins (m-way, m-pass, m-way+skew) with the checksum
+#   _ref/adb_ref_sort      sorting/ joins as the reference compiles them (the CPU baseline)
+TREE = _ref/src
+CKFLAGS = -std=c++14 -O3 -pthread -msse4.2 -mavx2 -w -I ref/stub -I ref
+HASH_SRC := $(wildcard $(TREE)/hashing/helper/*.cpp $(TREE)/hashing/joins/*.cpp $(TREE)/hashing/timer/*.cpp \
+                       $(TREE)/hashing/utils/*.cpp)
+HASH_SRC := $(filter-out %/fetcher_old.cpp,$(HASH_SRC))
+SORT_SRC := $(wildcard $(TREE)/sorting/affinity/*.cpp $(TREE)/sorting/datagen/*.cpp $(TREE)/sorting/joins/*.cpp \
+                       $(TREE)/sorting/timer/*.cpp $(TREE)/sorting/utils/*.cpp)
+HASH_CK_OBJ := $(patsubst $(TREE)/%.cpp,_ref/obj_ck/%.o,$(HASH_SRC))
+SORT_CK_OBJ := $(patsubst $(TREE)/%.cpp,_ref/obj_ck/%.o,$(SORT_SRC))
+SORT_OBJ := $(patsubst $(TREE)/%.cpp,_ref/obj/%.o,$(SORT_SRC))
+
+ck-all: _ref/adb_ref_ck_hash _ref/adb_ref_ck_sort _ref/adb_ref_sort
+
+_ref/obj_ck/hashing/%.o: $(TREE)/hashing/%.cpp ref/checksum.h
+	@mkdir -p $(dir $@)
+	$(CXX) $(CKFLAGS) -I $(TREE)/hashing -include ref/checksum.h -c $< -o $@
+
+_ref/obj_ck/sorting/%.o: $(TREE)/sorting/%.cpp ref/checksum.h
+	@mkdir -p $(dir $@)
+	$(CXX) $(CKFLAGS) -I $(TREE)/sorting -include ref/checksum.h -c $< -o $@
+
+_ref/obj/sorting/%.o: $(TREE)/sorting/%.cpp ref/checksum.h
+	@mkdir -p $(dir $@)
+	$(CXX) $(CKFLAGS) -DADB_REF_NO_CK -I $(TREE)/sorting -include ref/checksum.h -c $< -o $@
+
+_ref/obj_ck/harness_hash.o: ref/harness.cpp ref/gen.h ref/checksum.h
+	@mkdir -p $(dir $@)
+	$(CXX) $(CKFLAGS) -DADB_REF_CK -I $(TREE)/hashing -include ref/checksum.h -c $< -o $@
+
+_ref/obj_ck/harness_sort.o: ref/harness_sort.cpp ref/gen.h ref/checksum.h
+	@mkdir -p $(dir $@)
+	$(CXX) $(CKFLAGS) -DADB_REF_CK -I $(TREE)/sorting -include ref/checksum.h -c $< -o $@
+
+_ref/obj/harness_sort.o: ref/harness_sort.cpp ref/gen.h ref/checksum.h
+	@mkdir -p $(dir $@)
+	$(CXX) $(CKFLAGS) -DADB_REF_NO_CK -I $(TREE)/sorting -include ref/checksum.h -c $< -o $@
+
+_ref/adb_ref_ck_hash: $(HASH_CK_OBJ) _ref/obj_ck/harness_hash.o
+	$(CXX) -pthread -o $@ $^
+
+_ref/adb_ref_ck_sort: $(SORT_CK_OBJ) _ref/obj_ck/harness_sort.o
+	$(CXX) -pthread -o $@ $^
+
+_ref/adb_ref_sort: $(SORT_OBJ) _ref/obj/harness_sort.o
+	$(CXX) -pthread -o $@ $^
+
+.PHONY: ck-all

@@ -11,8 +11,9 @@
 //       restated here), `warmup` untimed calls (default 1 when reps > 1), then
 //       up to reps timed calls, stopping early once budget_s seconds of timed
 //       calls have run (at least one timed call)
-//   adb_ref_bench <algo> files <R.bin> <S.bin> <threads>
-//       relations from files of 8-byte {payload, key} tuples, one call
+//   adb_ref_bench <algo> files <R.bin> <S.bin> <threads> [progressive_step] [merge_step] [group_size]
+//       relations from files of 8-byte {payload, key} tuples, one call (the
+//       last three are param_t fields of the eager joins; defaults 1, 2, 2)
 //   adb_ref_bench dump <n> <theta> <R.bin> <S.bin>
 //       writes the relations that `gen` would join (to check the restated
 //       generator against the benchmark's)
@@ -44,6 +45,22 @@
 #include "joins/prj_params.h"
 #include "utils/generator.h"
 
+#ifdef ADB_REF_CK
+// Checksum build: the whole hashing/ tree prepared by oracle/ref/ref_tree.py is
+// linked (its own cpu mapping, generator globals and eager joins); the match
+// sites add into these accumulators (oracle/ref/checksum.h).
+#include "joins/onlinejoins.h"
+uint64_t adb_ref_checksum_total = 0;
+thread_local AdbRefAcc adb_ref_acc;
+thread_local bool adb_ref_probe_r = false;
+AdbRefAcc::~AdbRefAcc() { __atomic_fetch_add(&adb_ref_checksum_total, sum, __ATOMIC_RELAXED); }
+static void *alloc_aligned_rel(size_t size) {
+    void *p = nullptr;
+    if (posix_memalign(&p, 64, size)) return nullptr;
+    return p;
+}
+#define alloc_aligned alloc_aligned_rel
+#else
 int nthreads = 1;
 int numalocalize = 0;
 
@@ -57,127 +74,14 @@ void *alloc_aligned(size_t size) {
     if (posix_memalign(&p, 64, size)) return nullptr;
     return p;
 }
+#endif
 
-// ---- the benchmark generator (counter-based; see alliancedb_b200/csrc/datagen.cuh)
-static uint64_t fmix64(uint64_t z) {
-    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
-    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
-    return z ^ (z >> 31);
-}
-static uint64_t mix3(uint64_t seed, uint64_t stream, uint64_t i) {
-    return fmix64(fmix64(seed + stream * 0x632BE59BD9B4E019ULL) ^ (i * 0x9E3779B97F4A7C15ULL + 1));
-}
-struct Feistel {
-    uint64_t n, hmask;
-    uint32_t half;
-    uint64_t k[4];
-    Feistel(uint64_t n_, uint64_t seed) : n(n_) {
-        uint32_t bits = 2;
-        while (bits < 64 && (1ULL << bits) < n_) bits++;
-        bits = (bits + 1) & ~1u;
-        half = bits / 2;
-        hmask = (1ULL << half) - 1;
-        for (int r = 0; r < 4; r++) k[r] = mix3(seed, 1000 + r, 0);
-    }
-    uint64_t once(uint64_t x) const {
-        uint64_t L = x >> half, R = x & hmask;
-        for (int r = 0; r < 4; r++) {
-            const uint64_t t = R;
-            R = L ^ (fmix64(k[r] ^ R) & hmask);
-            L = t;
-        }
-        return (L << half) | R;
-    }
-    uint64_t operator()(uint64_t i) const {
-        uint64_t x = once(i);
-        while (x >= n) x = once(x);
-        return x;
-    }
-};
+#include "gen.h"
 
 static tuple_t *alloc_rel(uint64_t n) {
     // the reference allocates RELATION_PADDING of slack behind every relation,
     // which PRO uses as partitioning space (hashing/benchmark.cpp:15-17, 60)
     return (tuple_t *)alloc_aligned(n * sizeof(tuple_t) + RELATION_PADDING);
-}
-
-// Zipf(theta) rank in [0, n) by rejection-inversion (Hormann and Derflinger,
-// ACM TOMACS 6(3), 1996), as the benchmark generator draws it.
-struct ZipfRank {
-    double s, n, hx1, hn, sq;
-    static double helper1(double x) { return fabs(x) > 1e-8 ? log1p(x) / x : 1.0 - x * (0.5 - x * (1.0 / 3.0 - 0.25 * x)); }
-    static double helper2(double x) {
-        return fabs(x) > 1e-8 ? expm1(x) / x : 1.0 + x * 0.5 * (1.0 + x * (1.0 / 3.0) * (1.0 + 0.25 * x));
-    }
-    double h(double x) const { return exp(-s * log(x)); }
-    double hint(double x) const {
-        const double lx = log(x);
-        return helper2((1.0 - s) * lx) * lx;
-    }
-    double hinv(double x) const {
-        double t = x * (1.0 - s);
-        if (t < -1.0) t = -1.0;
-        return exp(helper1(t) * x);
-    }
-    ZipfRank(uint64_t n_, double theta) : s(theta), n((double)n_) {
-        hx1 = hint(1.5) - 1.0;
-        hn = hint(n + 0.5);
-        sq = 2.0 - hinv(hint(2.5) - h(2.0));
-    }
-    uint64_t sample(uint64_t seed, uint64_t j) const {
-        for (uint32_t attempt = 0; attempt < 64; attempt++) {
-            const double u01 = ((mix3(seed, 7, j * 64 + attempt) >> 11) + 1) * (1.0 / 9007199254740992.0);
-            const double u = hn + u01 * (hx1 - hn);
-            const double x = hinv(u);
-            double kd = floor(x + 0.5);
-            if (kd < 1.0) kd = 1.0;
-            if (kd > n) kd = n;
-            if (kd - x <= sq || u >= hint(kd + 0.5) - h(kd)) return (uint64_t)kd - 1;
-        }
-        return 0;
-    }
-};
-
-template <class F>
-static void par_for(uint64_t n, F f) {
-    unsigned nt = std::thread::hardware_concurrency();
-    if (nt == 0 || n < (1u << 16)) nt = 1;
-    std::vector<std::thread> th;
-    for (unsigned t = 0; t < nt; t++) {
-        const uint64_t b = n * t / nt, e = n * (t + 1) / nt;
-        th.emplace_back([=] { for (uint64_t i = b; i < e; i++) f(i); });
-    }
-    for (auto &x : th) x.join();
-}
-
-// R: key = 1 + perm_1(i), payload = i.  S: payload = j, key = R.key[idx_j], idx_j
-// uniform over 0..n-1 (theta 0) or rank_perm(Zipf(theta) rank) (seed 2).
-static void gen_pkfk(uint64_t n, double theta, std::vector<tuple_t> &R, std::vector<tuple_t> &S) {
-    R.resize(n);
-    S.resize(n);
-    Feistel perm(n ? n : 1, 1);
-    par_for(n, [&](uint64_t i) {
-        R[i].payloadID = (int32_t)i;
-        R[i].key = (int32_t)(1 + perm(i));
-    });
-    Feistel rank_perm(n ? n : 1, 2 ^ 0x5A5A5A5A5A5A5A5AULL);
-    ZipfRank z(n ? n : 1, theta > 0 ? theta : 1.0);
-    par_for(n, [&](uint64_t j) {
-        const uint64_t idx = theta > 0 ? rank_perm(z.sample(2, j))
-                                       : (uint64_t)(((unsigned __int128)mix3(2, 3, j) * n) >> 64);
-        S[j].payloadID = (int32_t)j;
-        S[j].key = R[idx].key;
-    });
-}
-
-static bool read_rel(const char *path, std::vector<tuple_t> &out) {
-    std::ifstream f(path, std::ios::binary | std::ios::ate);
-    if (!f) return false;
-    const std::streamsize bytes = f.tellg();
-    f.seekg(0);
-    out.resize(bytes / sizeof(tuple_t));
-    f.read(reinterpret_cast<char *>(out.data()), (std::streamsize)(out.size() * sizeof(tuple_t)));
-    return (bool)f;
 }
 
 typedef result_t *(*join_fn)(relation_t *, relation_t *, param_t);
@@ -186,6 +90,9 @@ typedef result_t *(*join_fn)(relation_t *, relation_t *, param_t);
 #include "joins/onlinejoins.h"
 extern "C" uint64_t adb_shim_checksum(const result_t *res);
 #endif
+#if defined(ADB_SHIM) || defined(ADB_REF_CK)
+#define ADB_ALL_HASHING_NAMES 1
+#endif
 
 static join_fn lookup(const std::string &algo) {
     static const struct {
@@ -193,9 +100,12 @@ static join_fn lookup(const std::string &algo) {
         join_fn fn;
     } table[] = {
         {"PRO", PRO}, {"PRH", PRH}, {"RJ_st", RJ_st}, {"NPO", NPO}, {"NPO_st", NPO_st},
-#ifdef ADB_SHIM
+#ifdef ADB_ALL_HASHING_NAMES
         {"PRHO", PRHO}, {"SHJ_st", SHJ_st}, {"SHJ_JM_NP", SHJ_JM_NP}, {"SHJ_JB_NP", SHJ_JB_NP},
-        {"SHJ_JBCR_NP", SHJ_JBCR_NP}, {"PMJ_st", PMJ_st}, {"PMJ_JM_NP", PMJ_JM_NP}, {"PMJ_JB_NP", PMJ_JB_NP},
+        {"SHJ_JBCR_NP", SHJ_JBCR_NP}, {"SHJ_HS_NP", SHJ_HS_NP}, {"PMJ_st", PMJ_st}, {"PMJ_JM_NP", PMJ_JM_NP},
+        {"PMJ_JB_NP", PMJ_JB_NP}, {"PMJ_JBCR_NP", PMJ_JBCR_NP}, {"PMJ_HS_NP", PMJ_HS_NP},
+#endif
+#ifdef ADB_SHIM
         {"RPJ_st", RPJ_st},
 #endif
     };
@@ -228,6 +138,7 @@ int main(int argc, char **argv) {
     }
     std::vector<tuple_t> R0, S0;
     int reps = 1, warmup = 0;
+    int progressive_step = 1, merge_step = 2, group_size = 2;
     double budget_s = 1e30;
     if (std::string(argv[2]) == "gen" && argc >= 6) {
         const double theta = argc >= 7 ? atof(argv[6]) : 0.0;
@@ -242,6 +153,9 @@ int main(int argc, char **argv) {
             return 2;
         }
         nthreads = atoi(argv[5]);
+        if (argc >= 7) progressive_step = atoi(argv[6]);
+        if (argc >= 8) merge_step = atoi(argv[7]);
+        if (argc >= 9) group_size = atoi(argv[8]);
     } else {
         return 2;
     }
@@ -250,10 +164,17 @@ int main(int argc, char **argv) {
     memset((void *)&p, 0, sizeof(p));
     p.nthreads = nthreads;
     p.duplicate_num = 1;
-    p.progressive_step = 1;
-    p.merge_step = 2;
+    p.progressive_step = progressive_step;
+    p.merge_step = merge_step;
+    p.group_size = group_size;
     tuple_t *rt = alloc_rel(R0.size()), *st = alloc_rel(S0.size());
     std::vector<double> ms;
+#ifdef ADB_REF_CK
+    std::vector<uint64_t> tsR(R0.size() + 1, 0), tsS(S0.size() + 1, 0);
+    bool ts_ok = true;
+    for (const auto &t : R0) ts_ok = ts_ok && (uint64_t)(uint32_t)t.payloadID < R0.size();
+    for (const auto &t : S0) ts_ok = ts_ok && (uint64_t)(uint32_t)t.payloadID < S0.size();
+#endif
     int64_t count = -1;
     uint64_t checksum = 0;
     double timed_s = 0;
@@ -262,6 +183,18 @@ int main(int argc, char **argv) {
         memcpy(rt, R0.data(), R0.size() * sizeof(tuple_t));
         memcpy(st, S0.data(), S0.size() * sizeof(tuple_t));
         relation_t relR{rt, R0.size(), nullptr}, relS{st, S0.size(), nullptr};
+#ifdef ADB_REF_CK
+        // arrival timestamps (all 0: every tuple has arrived when the join
+        // starts), read by the eager joins' fetchers only when WAIT is defined,
+        // at ts[payloadID]; attached only when every payload indexes its row
+        relation_payload_t payR{tsR.data(), R0.size()}, payS{tsS.data(), S0.size()};
+        if (ts_ok) {
+            relR.payload = &payR;
+            relS.payload = &payS;
+        }
+        adb_ref_checksum_total = 0;
+        adb_ref_acc.sum = 0;
+#endif
         const auto t0 = std::chrono::steady_clock::now();
         result_t *res = fn(&relR, &relS, p);
         const auto t1 = std::chrono::steady_clock::now();
@@ -272,6 +205,9 @@ int main(int argc, char **argv) {
         count = res->totalresults;
 #ifdef ADB_SHIM
         checksum = adb_shim_checksum(res);
+#endif
+#ifdef ADB_REF_CK
+        checksum = adb_ref_checksum_total + adb_ref_acc.sum;
 #endif
         free(res);
         if (r < warmup) continue;

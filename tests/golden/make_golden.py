@@ -1,14 +1,18 @@
 """Regenerate the golden fixtures under tests/golden/.
 
-Run on the machine that has the AllianceDB sources (the reference binary
-oracle/_ref/adb_ref_bench is built from them by `make -C oracle ref`):
+Run on the machine that has the AllianceDB sources (the reference binaries
+oracle/_ref/adb_ref_ck_{hash,sort} are built from them by
+`make -C oracle ck REF_ROOT=<AllianceDB tree>`):
 
     python tests/golden/make_golden.py
 
 Each case stores its relations (uint64 words key << 32 | payload, .npy) and, in
 cases.json, the expected match count and checksum:
-  * count_ref[algo]  the reference's own PRO / PRH / RJ_st / NPO / NPO_st run on
-                     the case (oracle/_ref/adb_ref_bench ... files ...);
+  * ref[label]       count and checksum of the reference's own join code run on
+                     the case (every hashing join but the HS model, which does
+                     not finish in this reference, and m-way / m-pass /
+                     m-way+skew), the checksum taken at the reference's match
+                     sites; or the error the reference run ended with;
   * count, checksum  the oracle's independent sort-based truth.
 The relations come from `gen_numpy`, a numpy restatement of the seeded
 generator of the library (alliancedb_b200/csrc/datagen.cuh); tests check that
@@ -116,11 +120,34 @@ def cases():
     return out
 
 
+# The reference's joins recorded per case: (label, binary, algorithm, threads).
+# Threads: 4 for the eager distribution models (JB / JBCR split work by
+# thread) and the partitioned joins; NPO at 1 thread (its multi-threaded build
+# loses tuples at random on repeated keys, so no fixture can hold it); the
+# sort-merge joins at 1 and at 4 threads.
+REF_RUNS = [(a, "hash", a, 4) for a in ("PRO", "PRH", "RJ_st", "NPO_st", "SHJ_st", "SHJ_JM_NP", "SHJ_JB_NP",
+                                        "SHJ_JBCR_NP", "PMJ_st", "PMJ_JM_NP", "PMJ_JB_NP", "PMJ_JBCR_NP")] + \
+           [("NPO@1", "hash", "NPO", 1)] + \
+           [(f"{a}@{t}", "sort", a, t) for a in ("m-way", "m-pass", "m-way+skew") for t in (1, 4)]
+REF_BIN = {"hash": ROOT / "oracle" / "_ref" / "adb_ref_ck_hash", "sort": ROOT / "oracle" / "_ref" / "adb_ref_ck_sort"}
+
+
+def run_ref(kind, algo, threads, rf, sf):
+    """One reference join on the relation files: {"count", "checksum"} or {"error"}."""
+    res = subprocess.run([str(REF_BIN[kind]), algo, "files", str(rf), str(sf), str(threads)], capture_output=True,
+                         text=True, timeout=120)
+    lines = [ln for ln in res.stdout.splitlines() if ln.startswith("{")]
+    if res.returncode != 0 or not lines:
+        return {"error": f"exit status {res.returncode}"}
+    d = json.loads(lines[-1])
+    return {"count": d["count"], "checksum": str(d["checksum"])}
+
+
 def main():
     from tests.oracle_bind import Oracle
-    ref = ROOT / "oracle" / "_ref" / "adb_ref_bench"
-    if not ref.exists():
-        sys.exit("oracle/_ref/adb_ref_bench is missing: run `make -C oracle ref` first")
+    for b in REF_BIN.values():
+        if not b.exists():
+            sys.exit(f"{b} is missing: run `make -C oracle ck REF_ROOT=<AllianceDB tree>` first")
     o = Oracle()
     meta = {}
     with tempfile.TemporaryDirectory() as tmp:
@@ -128,17 +155,12 @@ def main():
             np.save(HERE / f"{name}_R.npy", R)
             np.save(HERE / f"{name}_S.npy", S)
             count, checksum = o.truth(R, S)
-            ref_counts = {}
             rf, sf = Path(tmp) / "R.bin", Path(tmp) / "S.bin"
             R.tofile(rf)
             S.tofile(sf)
-            for algo in ("PRO", "PRH", "RJ_st", "NPO", "NPO_st"):
-                res = subprocess.run([str(ref), algo, "files", str(rf), str(sf), "4"], capture_output=True,
-                                     text=True, timeout=120)
-                if res.returncode == 0:
-                    ref_counts[algo] = json.loads(res.stdout.strip().splitlines()[-1])["count"]
+            ref = {label: run_ref(kind, algo, t, rf, sf) for label, kind, algo, t in REF_RUNS}
             meta[name] = {"n_r": int(len(R)), "n_s": int(len(S)), "count": count, "checksum": str(checksum),
-                          "count_ref": ref_counts}
+                          "ref": ref}
     (HERE / "cases.json").write_text(json.dumps(meta, indent=1, sort_keys=True) + "\n")
     print(json.dumps(meta, indent=1))
 

@@ -22,6 +22,8 @@ from tests.golden.make_golden import fmix64
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
 REF_BIN = Path(__file__).resolve().parent.parent / "oracle" / "_ref" / "adb_ref_bench"
+REF_CK_HASH = REF_BIN.parent / "adb_ref_ck_hash"
+REF_CK_SORT = REF_BIN.parent / "adb_ref_ck_sort"
 
 
 def pair_hash_np(key, rp, sp):
@@ -57,20 +59,47 @@ def test_pair_hash_matches_contract(oracle):
         assert oracle.pair_hash(int(k), int(r), int(s)) == int(pair_hash_np(k, r, s))
 
 
+# Where the reference's own join code does not return the true join on a golden
+# case.  Each entry is still checked: the recorded reference result must keep
+# differing from the truth in the way described (a fixture regenerated from a
+# fixed reference fails here and the entry goes).
+KNOWN_REF_DEFECTS = {
+    ("all_equal_200_300", "PMJ_st"):
+        "reports 209600 matches; its match sites see exactly the 60000 true pairs (checksum equal to the truth)",
+    **{("extreme_keys", a): "ends with a signal: keys >= 2^31 are negative int32 keys, which JB/JBCR's key % n "
+                            "and PMJ's sort/run code index with"
+       for a in ("SHJ_JB_NP", "SHJ_JBCR_NP", "PMJ_st", "PMJ_JM_NP", "PMJ_JB_NP", "PMJ_JBCR_NP")},
+    **{("non_pow2_1023_x_777", f"{a}@4"): "miscounts when the thread count does not divide |R| (correct at 1 thread)"
+       for a in ("m-way", "m-pass", "m-way+skew")},
+}
+
+
 def test_golden_fixtures(oracle):
+    """Truth, restatements and the reference's own joins agree on every fixture."""
     meta = json.loads((GOLDEN / "cases.json").read_text())
     assert set(meta) == set(golden_cases())
+    seen_defects = set()
     for name, m in meta.items():
         R = np.load(GOLDEN / f"{name}_R.npy")
         S = np.load(GOLDEN / f"{name}_S.npy")
         want = (m["count"], int(m["checksum"]))
         assert oracle.truth(R, S) == want, name
+        assert oracle.pk_truth(R, S) == want if len(np.unique(R >> np.uint64(32))) == len(R) else True
         assert oracle.pro(R, S) == want and oracle.npo(R, S) == want and oracle.smj(R, S) == want, name
         assert oracle.shj(R, S) == want and oracle.prh(R, S) == want, name
-        # the reference's own joins, run when the fixtures were made
-        assert m["count_ref"], name
-        for algo, c in m["count_ref"].items():
-            assert c == m["count"], (name, algo)
+        # the reference's own joins (count and match-site checksum), run when the fixtures were made
+        assert len(m["ref"]) == 19, name
+        for label, r in m["ref"].items():
+            got = (r.get("count"), int(r["checksum"]) if "checksum" in r else None)
+            if (name, label) in KNOWN_REF_DEFECTS:
+                seen_defects.add((name, label))
+                assert got != want, (name, label, "listed as a reference defect but now equals the truth")
+            else:
+                assert got == want, (name, label, r)
+    assert seen_defects == set(KNOWN_REF_DEFECTS)
+    # PMJ_st's miscount is in its reported count only
+    pmj = meta["all_equal_200_300"]["ref"]["PMJ_st"]
+    assert int(pmj["checksum"]) == int(meta["all_equal_200_300"]["checksum"])
 
 
 def test_golden_inputs_are_the_generators_output():
@@ -150,3 +179,33 @@ def test_reference_harness_generator_is_the_benchmarks(tmp_path, theta):
     S = adb.gen_fk(n, R, theta, 2)
     assert np.array_equal(np.fromfile(tmp_path / "R.bin", dtype=np.uint64), R.view(np.uint64))
     assert np.array_equal(np.fromfile(tmp_path / "S.bin", dtype=np.uint64), S.view(np.uint64))
+
+
+def _ref_ck(binary, algo, rf, sf, threads):
+    out = subprocess.run([str(binary), algo, "files", str(rf), str(sf), str(threads)], capture_output=True,
+                         text=True, timeout=300, check=True).stdout
+    d = json.loads([ln for ln in out.splitlines() if ln.startswith("{")][-1])
+    return d["count"], d["checksum"]
+
+
+@pytest.mark.skipif(not (REF_CK_HASH.exists() and REF_CK_SORT.exists()),
+                    reason="the reference's checksum builds exist only where its sources were")
+@pytest.mark.parametrize("theta", [0.0, 1.0])
+def test_reference_checksums_on_fresh_inputs(oracle, tmp_path, theta):
+    """The reference's own joins, checksum taken at their match sites, on a
+    foreign-key pair with Zipf-skewed S (not a fixture): every algorithm
+    equals the oracle's truth, and so do the oracle's restatements."""
+    n = 1 << 15
+    R = adb.gen_pk(n, 41)
+    S = adb.gen_fk(n + 1000, R, theta, 42)
+    R.tofile(tmp_path / "R.bin")
+    S.tofile(tmp_path / "S.bin")
+    want = oracle.truth(R, S)
+    rf, sf = tmp_path / "R.bin", tmp_path / "S.bin"
+    for algo in ("PRO", "PRH", "RJ_st", "NPO_st", "SHJ_st", "SHJ_JM_NP", "SHJ_JB_NP", "SHJ_JBCR_NP", "PMJ_st",
+                 "PMJ_JM_NP", "PMJ_JB_NP", "PMJ_JBCR_NP"):
+        assert _ref_ck(REF_CK_HASH, algo, rf, sf, 4) == want, algo
+    assert _ref_ck(REF_CK_HASH, "NPO", rf, sf, 1) == want
+    for algo in ("m-way", "m-pass", "m-way+skew"):
+        assert _ref_ck(REF_CK_SORT, algo, rf, sf, 4) == want, algo   # 4 divides |R|
+    assert oracle.pmj(R, S, n // 100, (n + 1000) // 100) == want
