@@ -17,11 +17,62 @@ workload generates its relations on the device from seeds unless stated.
 from __future__ import annotations
 
 import ctypes as C
+import json
+import os
+import subprocess
+import tempfile
 import time
+from pathlib import Path
 
 import numpy as np
 
 import alliancedb_b200 as adb
+
+ROOT = Path(__file__).resolve().parent.parent
+# algorithmic bytes per input tuple: partitioned (batched / served) 24, eager 16
+ALG_BYTES_PARTITIONED = 24
+ALG_BYTES_EAGER = 16
+
+
+def hbm_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text())["hbm_gbs"], "measured"
+    return 6650.0, "fallback"
+
+
+def roofline(tuples_per_s: float, bytes_per_tuple: int):
+    peak, kind = hbm_peak()
+    gbs = tuples_per_s * bytes_per_tuple / 1e9
+    return {"bound": "hbm", "alg_bytes_per_tuple": bytes_per_tuple, "achieved": gbs, "peak": peak,
+            "unit": "GB/s", "frac": gbs / peak, "peak_source": kind}
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def ref_windows(algo: str, windows, threads: int, binary: str = "adb_ref_bench"):
+    """The reference's own `algo` (oracle/_ref, compiled from its sources) on
+    each (R, S) window of `windows` in turn, one call per window, on this host:
+    returns the harness's JSON (tuples, count, summed call ms, tuples_per_s),
+    or None when the reference build is absent."""
+    ref = ROOT / "oracle" / "_ref" / binary
+    if not ref.exists() or not windows:
+        return None
+    with tempfile.TemporaryDirectory(dir=os.environ.get("ADB_TMP")) as tmp:
+        t = Path(tmp)
+        r_off = np.concatenate([[0], np.cumsum([len(r) for r, _ in windows])]).astype(np.uint64)
+        s_off = np.concatenate([[0], np.cumsum([len(s) for _, s in windows])]).astype(np.uint64)
+        np.concatenate([adb.as_words(r) for r, _ in windows]).tofile(t / "R.bin")
+        np.concatenate([adb.as_words(s) for _, s in windows]).tofile(t / "S.bin")
+        np.concatenate([r_off, s_off]).tofile(t / "off.bin")
+        out = subprocess.run([str(ref), algo, "windows", str(t / "R.bin"), str(t / "S.bin"), str(t / "off.bin"),
+                              str(threads)], capture_output=True, text=True, timeout=1800, check=True).stdout
+    return json.loads([ln for ln in out.splitlines() if ln.startswith("{")][-1])
 
 
 def _logu(rng, lo, hi, n):
@@ -57,7 +108,28 @@ def batch_windows(n_windows: int, lo: int, hi: int, seed: int):
     return dR.ptr, r_off, dS.ptr, s_off, keep
 
 
-def bench_batch(args):
+def _batch_cpu_sample(dR, r_off, dS, s_off, max_tuples=1 << 25, max_windows=256, seed=5):
+    """A seeded random sample of the batch's windows, copied to the host, of at
+    most max_windows windows and about max_tuples tuples."""
+    L = adb.lib()
+    rng = np.random.default_rng(seed)
+    out, total = [], 0
+    for w in rng.permutation(len(r_off) - 1):
+        nr, ns = int(r_off[w + 1] - r_off[w]), int(s_off[w + 1] - s_off[w])
+        if out and total + nr + ns > max_tuples:
+            continue
+        R = np.empty(nr, np.uint64)
+        S = np.empty(ns, np.uint64)
+        adb._check(L.adb_memcpy_d2h(R.ctypes.data, dR + int(r_off[w]) * 8, nr * 8))
+        adb._check(L.adb_memcpy_d2h(S.ctypes.data, dS + int(s_off[w]) * 8, ns * 8))
+        out.append((R, S))
+        total += nr + ns
+        if len(out) >= max_windows or total >= max_tuples:
+            break
+    return out
+
+
+def bench_batch(args, cpu: bool = True):
     lo, hi = 10, 22
     dR, r_off, dS, s_off, keep = batch_windows(args.windows, lo, hi, 11)
     tuples = int(r_off[-1] + s_off[-1])
@@ -72,34 +144,68 @@ def bench_batch(args):
     assert np.array_equal(c1, c0) and np.array_equal(k1, k0), "per-window and batched results differ"
     best0 = float(np.median(ms0))
     v0, v1 = tuples / (best0 / 1e3), tuples / (ms1 / 1e3)
-    return {"metric": "batched windows join input tuples/s", "value": v0, "unit": "tuples/s",
-            "higher_is_better": True, "n_gpus": 1, "data": "synthetic",
-            "config": {"workload": f"{args.windows} window pairs, sizes log-uniform [2^{lo}, 2^{hi}] per side, "
-                                   "keys uniform over 4x window size, 25% windows Zipf 0.8",
-                       "windows": args.windows, "tuples": tuples},
-            "ms_batched": best0, "ms_per_window_launches": ms1, "per_window_value": v1,
-            "speedup_batched_vs_per_window": v0 / v1, "matches": int(c0.sum()),
-            "fanout_bits_by_size_bucket": table[lo:hi + 1]}
+    out = {"metric": "batched windows join input tuples/s", "value": v0, "unit": "tuples/s",
+           "higher_is_better": True, "n_gpus": 1, "data": "synthetic",
+           "config": {"workload": f"{args.windows} window pairs, sizes log-uniform [2^{lo}, 2^{hi}] per side, "
+                                  "keys uniform over 4x window size, 25% windows Zipf 0.8",
+                      "windows": args.windows, "tuples": tuples},
+           "ms_batched": best0, "ms_per_window_launches": ms1, "per_window_value": v1,
+           "speedup_batched_vs_per_window": v0 / v1, "matches": int(c0.sum()),
+           "roofline": roofline(v0, ALG_BYTES_PARTITIONED),
+           "fanout_bits_by_size_bucket": table[lo:hi + 1]}
+    if cpu:
+        sample = _batch_cpu_sample(dR, r_off, dS, s_off)
+        th = host_threads()
+        d = ref_windows("PRO", sample, th)
+        if d is not None:
+            out["cpu_baseline"] = {"value": d["tuples_per_s"], "unit": "tuples/s", "cores": th, "kind": "reference",
+                                   "sample": f"reference PRO run per window, one window after the other, on "
+                                             f"{d['windows']} windows ({d['tuples']} tuples) drawn at random from "
+                                             f"the batch, {th} threads; {d['count']} matches"}
+    del keep
+    return out
 
 
-def bench_serve(args):
-    rng = np.random.default_rng(21)
-    n = args.requests
+def serve_requests(n: int, seed: int = 21):
+    rng = np.random.default_rng(seed)
     t = np.cumsum(rng.exponential(1e6 / 2000.0, size=n))
     nr = _logu(rng, 12, 24, n)
     ns = _logu(rng, 12, 24, n)
-    reqs = [(int(t[i]), int(nr[i]), int(ns[i]), 5000 + i) for i in range(n)]
+    return [(int(t[i]), int(nr[i]), int(ns[i]), 5000 + i) for i in range(n)], t, nr, ns
+
+
+def bench_serve(args, cpu: bool = True):
+    n = args.requests
+    reqs, t, nr, ns = serve_requests(n)
     adb.serve_run(reqs[:50], budget_bytes=120 << 30, max_batch=256, realtime=False)   # warm-up
     res, st = adb.serve_run(reqs, budget_bytes=120 << 30, max_batch=256, realtime=True)
     assert all(r.status == 0 and r.count == reqs[i][2] for i, r in enumerate(res))
-    return {"metric": "served join input tuples/s", "value": st.tuples_per_s, "unit": "tuples/s",
-            "higher_is_better": True, "n_gpus": 1, "data": "synthetic",
-            "config": {"workload": f"{n} requests, Poisson 2000 req/s, sizes log-uniform [2^12, 2^24] per side, "
-                                   "FK uniform keys, budget 120 GB", "requests": n},
-            "latency_ms": {"p50": st.p50_ms, "p99": st.p99_ms, "p999": st.p999_ms},
-            "batches": int(st.batches), "mean_batch": st.mean_batch, "makespan_ms": st.makespan_ms,
-            "offered_tuples_per_s": float((nr + ns).sum() / (t[-1] / 1e6)),
-            "peak_arena_gb": st.peak_arena_bytes / 2**30}
+    out = {"metric": "served join input tuples/s", "value": st.tuples_per_s, "unit": "tuples/s",
+           "higher_is_better": True, "n_gpus": 1, "data": "synthetic",
+           "config": {"workload": f"{n} requests, Poisson 2000 req/s, sizes log-uniform [2^12, 2^24] per side, "
+                                  "FK uniform keys, budget 120 GB", "requests": n},
+           "latency_ms": {"p50": st.p50_ms, "p99": st.p99_ms, "p999": st.p999_ms},
+           "batches": int(st.batches), "mean_batch": st.mean_batch, "makespan_ms": st.makespan_ms,
+           "offered_tuples_per_s": float((nr + ns).sum() / (t[-1] / 1e6)),
+           "roofline": roofline(st.tuples_per_s, ALG_BYTES_PARTITIONED),
+           "peak_arena_gb": st.peak_arena_bytes / 2**30}
+    if cpu:
+        # the first requests, generated on the host exactly as the device generates them
+        sample, total = [], 0
+        for (_, a, b, seed) in reqs:
+            if sample and total + a + b > (1 << 26):
+                break
+            R = adb.gen_pk(a, seed)
+            sample.append((R, adb.gen_fk(b, R, 0.0, seed + 1)))
+            total += a + b
+        th = host_threads()
+        d = ref_windows("PRO", sample, th)
+        if d is not None:
+            out["cpu_baseline"] = {"value": d["tuples_per_s"], "unit": "tuples/s", "cores": th, "kind": "reference",
+                                   "sample": f"reference PRO run per request, one after the other (no arrival "
+                                             f"gaps), on the first {d['windows']} requests ({d['tuples']} tuples), "
+                                             f"{th} threads; {d['count']} matches"}
+    return out
 
 
 def make_streams(seconds: float, rate_per_s: float, key_space: int, dup: int, seed: int):
@@ -117,7 +223,7 @@ def make_streams(seconds: float, rate_per_s: float, key_space: int, dup: int, se
     return out
 
 
-def bench_stream(args):
+def bench_stream(args, cpu: bool = True):
     R, S = make_streams(8.0, 1.6e6, 1 << 20, 4, 31)
     out = {"metric": "stream join input tuples/s", "unit": "tuples/s", "higher_is_better": True, "n_gpus": 1,
            "data": "synthetic",
@@ -150,4 +256,42 @@ def bench_stream(args):
                              "p95": float(np.median([g.lat_p95 for g in prog])),
                              "p99": float(np.median([g.lat_p99 for g in prog]))}}
     out["value"] = out["SHJ_JM_NP"]["tuples_per_s"]
+    out["roofline"] = roofline(out["value"], ALG_BYTES_EAGER)
+    if cpu:
+        # the reference's eager joins on the first window (WAIT off: every tuple
+        # has arrived, the throughput configuration), one call per algorithm
+        r0, s0 = R[R["ts_ms"] < 1000], S[S["ts_ms"] < 1000]
+        w0 = [(adb.tuples(r0["key"], r0["payload"]), adb.tuples(s0["key"], s0["payload"]))]
+        th = host_threads()
+        base = {}
+        for algo in ("SHJ_JM_NP", "SHJ_JBCR_NP", "PMJ_JM_NP", "PMJ_JBCR_NP"):
+            d = ref_windows(algo, w0, th, "adb_ref_hash")
+            if d is not None:
+                base[algo] = {"value": d["tuples_per_s"], "count": d["count"]}
+        if base:
+            out["cpu_baseline"] = {"value": base.get("SHJ_JM_NP", {}).get("value"), "unit": "tuples/s",
+                                   "cores": th, "kind": "reference", "per_algorithm": base,
+                                   "sample": f"the reference's eager joins (WAIT off: throughput) on the first "
+                                             f"1000 ms window ({len(w0[0][0])} + {len(w0[0][1])} tuples), one call "
+                                             f"each, {th} threads"}
     return out
+
+
+def forms_summary(args):
+    """Compact C3 / C4 / C5 results for the default benchmark line."""
+    b = bench_batch(args)
+    sv = bench_serve(args)
+    st = bench_stream(args)
+    keep = ("value", "unit", "roofline", "cpu_baseline", "config")
+    return {
+        "batch": {**{k: b[k] for k in keep if k in b}, "per_window_value": b["per_window_value"],
+                  "speedup_batched_vs_per_window": b["speedup_batched_vs_per_window"],
+                  "ms_batched": b["ms_batched"], "ms_per_window_launches": b["ms_per_window_launches"]},
+        "serve": {**{k: sv[k] for k in keep if k in sv}, "latency_ms": sv["latency_ms"],
+                  "offered_tuples_per_s": sv["offered_tuples_per_s"], "mean_batch": sv["mean_batch"]},
+        "stream": {**{k: st[k] for k in keep if k in st}, "algorithm": "SHJ_JM_NP",
+                   "per_algorithm_tuples_per_s": {a: st[a]["tuples_per_s"] for a in ("SHJ_JM_NP", "SHJ_JB_NP",
+                                                                                       "PMJ_JM_NP")},
+                   "realtime_window_latency_ms": st["SHJ_JM_NP_realtime"]["window_latency_ms"],
+                   "realtime_match_latency_ms": st["SHJ_JM_NP_realtime"]["match_latency_ms"]},
+    }

@@ -14,8 +14,11 @@ checksum.  A step = one join of the full relations.
           inside every timed step
   roofline  the dominant kernel's algorithmic bytes / its device time vs the
           measured HBM copy bandwidth (MEASURED_PEAKS.json)
-  cpu_baseline  the CPU join timed on this host (rank 0, N=1) on a bounded
-          sample of the workload
+  cpu_baseline  the reference's CPU join timed on this host (rank 0, N=1) on
+          the same workload
+  batch / serve / stream  (rank 0, N=1) the batched-windows, serving-loop and
+          eager stream-join forms: tuples/s, HBM roofline fraction, latency
+          percentiles, and the reference's CPU code on a stated sample
 
 `--impl reference` times the reference CPU join of the same workload instead:
 the reference's own code compiled from its sources (oracle/_ref) when present,
@@ -274,6 +277,8 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=120.0,
                     help="--impl reference: stop timing once this many seconds of calls have run")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the batched / served / stream sub-objects of the default line")
     ap.add_argument("--workload", default="join", choices=["join", "batch", "serve", "stream"],
                     help="join: one R/S pair (default, the headline); batch: 4096 windows, one launch "
                          "sequence vs one per window; serve: open-loop requests, p50/p99/p999; "
@@ -433,6 +438,15 @@ def main():
             line["cpu_baseline"] = {"value": v, "unit": "tuples/s", "cores": 1, "kind": "port",
                                     "sample": f"oracle {args.algo} restatement on the full workload "
                                               f"(|R|=|S|=2^{args.log2n}, theta={args.theta}), {reps} calls"}
+    if rank == 0 and world == 1 and not args.no_forms:
+        # the batched, served and stream forms of the same join library
+        # (batched windows, serving loop, eager stream joins), each with its own
+        # roofline and CPU baseline, outside the timed region above
+        from alliancedb_b200 import workloads
+        del dR, dS
+        torch.cuda.empty_cache()
+        fargs = argparse.Namespace(**{**vars(args), "steps": 6})
+        line.update(workloads.forms_summary(fargs))
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

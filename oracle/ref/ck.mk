@@ -3,6 +3,7 @@
 #   _ref/adb_ref_ck_hash   hashing/ joins (PRO ... PMJ_*) with the checksum at the match sites
 #   _ref/adb_ref_ck_sort   sorting/ joins (m-way, m-pass, m-way+skew) with the checksum
 #   _ref/adb_ref_sort      sorting/ joins as the reference compiles them (the CPU baseline)
+#   _ref/adb_ref_hash      hashing/ joins as the reference compiles them (the eager joins' CPU baseline)
 TREE = _ref/src
 CKFLAGS = -std=c++14 -O3 -pthread -msse4.2 -mavx2 -w -I ref/stub -I ref
 HASH_SRC := $(wildcard $(TREE)/hashing/helper/*.cpp $(TREE)/hashing/joins/*.cpp $(TREE)/hashing/timer/*.cpp \
@@ -13,8 +14,9 @@ SORT_SRC := $(wildcard $(TREE)/sorting/affinity/*.cpp $(TREE)/sorting/datagen/*.
 HASH_CK_OBJ := $(patsubst $(TREE)/%.cpp,_ref/obj_ck/%.o,$(HASH_SRC))
 SORT_CK_OBJ := $(patsubst $(TREE)/%.cpp,_ref/obj_ck/%.o,$(SORT_SRC))
 SORT_OBJ := $(patsubst $(TREE)/%.cpp,_ref/obj/%.o,$(SORT_SRC))
+HASH_OBJ := $(patsubst $(TREE)/%.cpp,_ref/obj/%.o,$(HASH_SRC))
 
-ck-all: _ref/adb_ref_ck_hash _ref/adb_ref_ck_sort _ref/adb_ref_sort
+ck-all: _ref/adb_ref_ck_hash _ref/adb_ref_ck_sort _ref/adb_ref_sort _ref/adb_ref_hash
 
 _ref/obj_ck/hashing/%.o: $(TREE)/hashing/%.cpp ref/checksum.h
 	@mkdir -p $(dir $@)
@@ -23,6 +25,17 @@ _ref/obj_ck/hashing/%.o: $(TREE)/hashing/%.cpp ref/checksum.h
 _ref/obj_ck/sorting/%.o: $(TREE)/sorting/%.cpp ref/checksum.h
 	@mkdir -p $(dir $@)
 	$(CXX) $(CKFLAGS) -I $(TREE)/sorting -include ref/checksum.h -c $< -o $@
+
+_ref/obj/hashing/%.o: $(TREE)/hashing/%.cpp ref/checksum.h
+	@mkdir -p $(dir $@)
+	$(CXX) $(CKFLAGS) -DADB_REF_NO_CK -I $(TREE)/hashing -include ref/checksum.h -c $< -o $@
+
+_ref/obj/harness_hash.o: ref/harness.cpp ref/gen.h ref/checksum.h
+	@mkdir -p $(dir $@)
+	$(CXX) $(CKFLAGS) -DADB_REF_FULL -DADB_REF_NO_CK -I $(TREE)/hashing -include ref/checksum.h -c $< -o $@
+
+_ref/adb_ref_hash: $(HASH_OBJ) _ref/obj/harness_hash.o
+	$(CXX) -pthread -o $@ $^
 
 _ref/obj/sorting/%.o: $(TREE)/sorting/%.cpp ref/checksum.h
 	@mkdir -p $(dir $@)

@@ -14,14 +14,18 @@
 //   adb_ref_bench <algo> files <R.bin> <S.bin> <threads> [progressive_step] [merge_step] [group_size]
 //       relations from files of 8-byte {payload, key} tuples, one call (the
 //       last three are param_t fields of the eager joins; defaults 1, 2, 2)
+//   adb_ref_bench <algo> windows <R.bin> <S.bin> <off.bin> <threads>
+//       many independent R/S window pairs joined one after the other (below)
 //   adb_ref_bench dump <n> <theta> <R.bin> <S.bin>
 //       writes the relations that `gen` would join (to check the restated
 //       generator against the benchmark's)
 // Prints one JSON line: algo, n_r, n_s, threads, count, ms (median), reps (timed
 // calls made), tuples_per_s.
 //
-// Built twice by oracle/Makefile: adb_ref_bench links the reference's join
-// objects; adb_ref_bench_gpu (ADB_SHIM defined) links the same calls against
+// Built by oracle/Makefile: adb_ref_bench links the reference's PRO / NPO join
+// objects; adb_ref_hash (ADB_REF_FULL) and adb_ref_ck_hash (ADB_REF_CK, with the
+// checksum) link the whole prepared hashing/ tree, eager joins included;
+// adb_ref_bench_gpu (ADB_SHIM defined) links the same calls against
 // alliancedb_b200/shim/reference_shim.cpp + libadb_b200.so instead, i.e. the
 // reference's call sites running the GPU library through the reference's
 // function signatures, and also prints the result's checksum.
@@ -46,14 +50,20 @@
 #include "utils/generator.h"
 
 #ifdef ADB_REF_CK
-// Checksum build: the whole hashing/ tree prepared by oracle/ref/ref_tree.py is
-// linked (its own cpu mapping, generator globals and eager joins); the match
-// sites add into these accumulators (oracle/ref/checksum.h).
+#define ADB_REF_FULL 1
+#endif
+
+#ifdef ADB_REF_FULL
+// Whole-tree builds: the hashing/ tree prepared by oracle/ref/ref_tree.py is
+// linked (its own cpu mapping, generator globals and eager joins).  With
+// ADB_REF_CK its match sites add into these accumulators (oracle/ref/checksum.h).
 #include "joins/onlinejoins.h"
+#ifdef ADB_REF_CK
 uint64_t adb_ref_checksum_total = 0;
 thread_local AdbRefAcc adb_ref_acc;
 thread_local bool adb_ref_probe_r = false;
 AdbRefAcc::~AdbRefAcc() { __atomic_fetch_add(&adb_ref_checksum_total, sum, __ATOMIC_RELAXED); }
+#endif
 static void *alloc_aligned_rel(size_t size) {
     void *p = nullptr;
     if (posix_memalign(&p, 64, size)) return nullptr;
@@ -90,7 +100,7 @@ typedef result_t *(*join_fn)(relation_t *, relation_t *, param_t);
 #include "joins/onlinejoins.h"
 extern "C" uint64_t adb_shim_checksum(const result_t *res);
 #endif
-#if defined(ADB_SHIM) || defined(ADB_REF_CK)
+#if defined(ADB_SHIM) || defined(ADB_REF_FULL)
 #define ADB_ALL_HASHING_NAMES 1
 #endif
 
@@ -112,6 +122,61 @@ static join_fn lookup(const std::string &algo) {
     for (const auto &e : table)
         if (algo == e.name) return e.fn;
     return nullptr;
+}
+
+// `windows` mode: window w is R[r_off[w], r_off[w+1]) joined with
+// S[s_off[w], s_off[w+1]) (off.bin: the W+1 entries of r_off, then the W+1 of
+// s_off, as u64), joined one after the other by one call each, the way a
+// per-window CPU deployment of the reference runs them.  Times every call
+// (fresh copies of the window outside the timed part) and prints the sum of
+// counts and of the call times.
+static int run_windows(join_fn fn, const std::string &algo, char **argv) {
+    std::vector<tuple_t> R0, S0;
+    std::vector<uint64_t> off;
+    if (!read_rel(argv[3], R0) || !read_rel(argv[4], S0)) return 2;
+    {
+        std::ifstream f(argv[5], std::ios::binary | std::ios::ate);
+        if (!f) return 2;
+        off.resize((size_t)f.tellg() / 8);
+        f.seekg(0);
+        f.read(reinterpret_cast<char *>(off.data()), (std::streamsize)(off.size() * 8));
+    }
+    nthreads = std::max(1, atoi(argv[6]));
+    const size_t W = off.size() / 2 - 1;
+    const uint64_t *r_off = off.data(), *s_off = off.data() + W + 1;
+    param_t p;
+    memset((void *)&p, 0, sizeof(p));
+    p.nthreads = nthreads;
+    p.duplicate_num = 1;
+    p.progressive_step = 1;
+    p.merge_step = 2;
+    p.group_size = 2;
+    uint64_t maxr = 0, maxs = 0;
+    for (size_t w = 0; w < W; w++) {
+        maxr = std::max(maxr, r_off[w + 1] - r_off[w]);
+        maxs = std::max(maxs, s_off[w + 1] - s_off[w]);
+    }
+    tuple_t *rt = alloc_rel(maxr), *st = alloc_rel(maxs);
+    double ms = 0;
+    int64_t count = 0;
+    for (size_t w = 0; w < W; w++) {
+        const uint64_t nr = r_off[w + 1] - r_off[w], ns = s_off[w + 1] - s_off[w];
+        memcpy(rt, R0.data() + r_off[w], nr * sizeof(tuple_t));
+        memcpy(st, S0.data() + s_off[w], ns * sizeof(tuple_t));
+        relation_t relR{rt, nr, nullptr}, relS{st, ns, nullptr};
+        const auto t0 = std::chrono::steady_clock::now();
+        result_t *res = fn(&relR, &relS, p);
+        const auto t1 = std::chrono::steady_clock::now();
+        if (!res) return 1;
+        count += res->totalresults;
+        free(res);
+        ms += std::chrono::duration<double, std::milli>(t1 - t0).count();
+    }
+    printf("{\"algo\": \"%s\", \"windows\": %zu, \"tuples\": %llu, \"threads\": %d, \"count\": %lld, "
+           "\"ms\": %.3f, \"tuples_per_s\": %.1f}\n",
+           algo.c_str(), W, (unsigned long long)(r_off[W] + s_off[W]), nthreads, (long long)count, ms,
+           (r_off[W] + s_off[W]) / (ms / 1e3));
+    return 0;
 }
 
 int main(int argc, char **argv) {
@@ -136,6 +201,7 @@ int main(int argc, char **argv) {
         fprintf(stderr, "unsupported algorithm %s\n", algo.c_str());
         return 2;
     }
+    if (std::string(argv[2]) == "windows" && argc >= 7) return run_windows(fn, algo, argv);
     std::vector<tuple_t> R0, S0;
     int reps = 1, warmup = 0;
     int progressive_step = 1, merge_step = 2, group_size = 2;
@@ -169,7 +235,7 @@ int main(int argc, char **argv) {
     p.group_size = group_size;
     tuple_t *rt = alloc_rel(R0.size()), *st = alloc_rel(S0.size());
     std::vector<double> ms;
-#ifdef ADB_REF_CK
+#ifdef ADB_REF_FULL
     std::vector<uint64_t> tsR(R0.size() + 1, 0), tsS(S0.size() + 1, 0);
     bool ts_ok = true;
     for (const auto &t : R0) ts_ok = ts_ok && (uint64_t)(uint32_t)t.payloadID < R0.size();
@@ -183,7 +249,7 @@ int main(int argc, char **argv) {
         memcpy(rt, R0.data(), R0.size() * sizeof(tuple_t));
         memcpy(st, S0.data(), S0.size() * sizeof(tuple_t));
         relation_t relR{rt, R0.size(), nullptr}, relS{st, S0.size(), nullptr};
-#ifdef ADB_REF_CK
+#ifdef ADB_REF_FULL
         // arrival timestamps (all 0: every tuple has arrived when the join
         // starts), read by the eager joins' fetchers only when WAIT is defined,
         // at ts[payloadID]; attached only when every payload indexes its row
@@ -192,6 +258,8 @@ int main(int argc, char **argv) {
             relR.payload = &payR;
             relS.payload = &payS;
         }
+#endif
+#ifdef ADB_REF_CK
         adb_ref_checksum_total = 0;
         adb_ref_acc.sum = 0;
 #endif
