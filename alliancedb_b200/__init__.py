@@ -153,6 +153,7 @@ _SIGS = {
                                 C.POINTER(ServeResult), C.POINTER(ServeStats)]),
     "adb_batch_set_tuning": (C.c_int, [C.POINTER(C.c_int)]),
     "adb_npo_join_noalloc": (C.c_int, [_P, _U64, _P, _U64, _P, _P]),
+    "adb_shard_split": (C.c_int, [_P, _U64, C.c_uint32, _P, C.POINTER(C.c_uint64), _P]),
     "adb_device_alloc": (C.c_int, [C.POINTER(C.c_void_p), C.c_size_t]),
     "adb_device_free": (C.c_int, [_P]),
     "adb_host_alloc_pinned": (C.c_int, [C.POINTER(C.c_void_p), C.c_size_t]),

@@ -16,12 +16,21 @@
 //        and shuffler.cpp:20-168 decide which worker sees which tuple; every model
 //        yields the same matches (all twelve variants return equal counts).
 //
-// Device design.  Tuples arrive in micro-batches (batch_tuples per side).
-//   SHJ: per window two open-addressing tables HR, HS in device memory (tuple
-//        words as slots, one 64-bit CAS per insert, as in npo_join.cuh).  A batch
-//        runs two launches: R_b inserts into HR and probes HS, then S_b inserts
-//        into HS and probes HR, so every (r, s) pair is found exactly once, by
-//        whichever of the two arrived later (same batch: by s).  The models map
+// Device design.  Tuples arrive in micro-batches (batch_tuples per side); in
+// arrival order batch b of R comes before batch b of S (shj() alternates R and
+// S), and a pair (r, s) belongs to whichever of the two arrived later.
+//   SHJ: per window two open-addressing tables HR, HS in device memory of
+//        16-byte records {tuple word, arrival batch}, a record claimed by one
+//        32-bit CAS on its batch field (every tuple value can be stored).
+//        With arrivals released in real time (realtime = 1), or with progress
+//        stamps, each batch runs two launches: R_b inserts into HR and probes
+//        HS, then S_b inserts into HS and probes HR, so every pair is found
+//        once, by its later tuple.  Otherwise (the throughput configuration,
+//        the reference's WAIT undefined) a window runs two launches in all:
+//        every tuple of both sides is inserted, then every tuple probes the
+//        other side's table and keeps only the tuples that arrived before it
+//        (an S tuple: R batches <= its own; an R tuple: S batches < its own) --
+//        the same pairs, each found once by its later tuple.  The models map
 //        to the table layout: JM (R replicated, S split) and HS use one shared
 //        table per side; JB (key-hash routing to nthreads joiners) splits each
 //        table into nthreads key-hash sub-tables; JBCR (groups of group_size
@@ -32,7 +41,9 @@
 //        itself (the initial-run join) and, merge-path style, with the sorted
 //        accumulation of all earlier runs of the other side (the merged-run
 //        join, done eagerly as each run arrives), then merged into its side's
-//        accumulation.
+//        accumulation.  adb_stream_join without real-time release or progress
+//        stamps (the throughput configuration) joins a window as one run: its
+//        matches are the same, and progressiveness needs arrival gating.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -50,60 +61,104 @@ enum { M_JM_NP = 0, M_JM_P = 1, M_JB_NP = 2, M_JB_P = 3, M_JBCR_NP = 4, M_JBCR_P
 // ---------------------------------------------------------------------------
 // SHJ
 // ---------------------------------------------------------------------------
+constexpr uint32_t kNoBatch = 0xFFFFFFFFu;   // batch field of an empty record
+
 struct ShjTables {
-    uint64_t *tab[2];          // R, S
+    ulonglong2 *tab[2];        // R, S: records {x = tuple word, y = arrival batch (low 32 bits)}
     uint32_t log2sub[2];       // slots per sub-table (log2)
     uint32_t log2parts;        // sub-tables per side (log2)
-    unsigned long long *sent;  // [2] tuples equal to the empty marker, per side
 };
 
 __device__ __forceinline__ uint32_t shj_part(uint32_t key, uint32_t log2parts) {
     return log2parts ? (uint32_t)((key * 0x85EBCA6Bu) >> (32 - log2parts)) : 0u;
 }
 
-// One micro-batch of one side: insert into the own table, probe the other.
-// `in` holds elements of `stride` 64-bit words with the tuple in the last word
-// (1: plain tuples, 2: adb_stream_tuple).
-__global__ void shj_batch(const uint64_t *__restrict__ in, uint32_t stride, uint64_t n, int side, ShjTables t,
-                          unsigned long long *acc, int *err) {
+// Inserts tuple word w of arrival batch `batch` into side `side`'s table.
+__device__ __forceinline__ void shj_insert(const ShjTables &t, int side, uint64_t w, uint32_t batch, int *err) {
+    const uint32_t lo = t.log2sub[side];
+    const uint64_t m = (1ULL << lo) - 1;
+    const uint32_t key = tkey(w);
+    ulonglong2 *tab = t.tab[side] + ((uint64_t)shj_part(key, t.log2parts) << lo);
+    uint64_t slot = npo_hash(key, lo);
+    for (uint64_t tries = 0;; tries++) {
+        unsigned int *bf = reinterpret_cast<unsigned int *>(&tab[slot].y);
+        if (atomicCAS(bf, kNoBatch, batch) == kNoBatch) {
+            tab[slot].x = w;
+            return;
+        }
+        slot = (slot + 1) & m;
+        if (tries > m) { atomicExch(err, 2); return; }   // table full: cannot happen at load <= 0.5
+    }
+}
+
+// Probes side `side`'s table with tuple word w (of the other side) and adds the
+// matches whose arrival batch is <= max_batch.  r_probe: w is an R tuple.
+__device__ __forceinline__ void shj_probe(const ShjTables &t, int side, uint64_t w, uint32_t max_batch, bool r_probe,
+                                          Acc &a) {
+    const uint32_t lo = t.log2sub[side];
+    const uint64_t m = (1ULL << lo) - 1;
+    const uint32_t key = tkey(w);
+    const ulonglong2 *tab = t.tab[side] + ((uint64_t)shj_part(key, t.log2parts) << lo);
+    uint64_t slot = npo_hash(key, lo);
+    for (uint64_t tries = 0; tries <= m; tries++) {
+        const ulonglong2 rec = tab[slot];
+        const uint32_t b = (uint32_t)rec.y;
+        if (b == kNoBatch) break;
+        if (tkey(rec.x) == key && b <= max_batch) {
+            a.count++;
+            a.sum += r_probe ? pair_hash(key, tpay(w), tpay(rec.x)) : pair_hash(key, tpay(rec.x), tpay(w));
+        }
+        slot = (slot + 1) & m;
+    }
+}
+
+// One micro-batch of one side (per-batch form): insert into the own table,
+// probe the other (which holds only earlier arrivals).  `in` holds elements of
+// `stride` 64-bit words with the tuple in the last word (1: plain tuples, 2:
+// adb_stream_tuple).
+__global__ void shj_batch(const uint64_t *__restrict__ in, uint32_t stride, uint64_t n, int side, uint32_t batch,
+                          ShjTables t, unsigned long long *acc, int *err) {
     __shared__ uint64_t red[64];
-    const int own = side, oth = 1 - side;
-    const uint32_t lo = t.log2sub[own], lt = t.log2sub[oth];
-    const uint64_t mown = (1ULL << lo) - 1, moth = (1ULL << lt) - 1;
-    const uint64_t nsent_oth = t.sent[oth];
     Acc a;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t w = in[i * stride + (stride - 1)];
-        const uint32_t key = tkey(w);
-        // (1)/(3): insert into the own side's table
-        if (w == kEmpty) {
-            atomicAdd(&t.sent[own], 1ull);
+        shj_insert(t, side, w, batch, err);                         // (1)/(3)
+        shj_probe(t, 1 - side, w, kNoBatch - 1, side == 0, a);     // (2)/(4)
+    }
+    block_flush(a, acc, red);
+}
+
+// Throughput form, step 1: every tuple of the window (R tuples 0 .. nR - 1,
+// then S tuples) into its side's table with its arrival batch (index / step).
+__global__ void shj_insert_window(const uint64_t *__restrict__ R, uint64_t nR, const uint64_t *__restrict__ S,
+                                  uint64_t nS, uint32_t stride, uint64_t sr, uint64_t ss, ShjTables t, int *err) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nR + nS;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const bool isr = i < nR;
+        const uint64_t k = isr ? i : i - nR;
+        const uint64_t w = (isr ? R : S)[k * stride + (stride - 1)];
+        shj_insert(t, isr ? 0 : 1, w, (uint32_t)(k / (isr ? sr : ss)), err);
+    }
+}
+
+// Throughput form, step 2: every tuple probes the other side's table for the
+// tuples that arrived before it: an S tuple of batch b meets R batches <= b,
+// an R tuple of batch b meets S batches < b (R batch b is released first).
+__global__ void shj_probe_window(const uint64_t *__restrict__ R, uint64_t nR, const uint64_t *__restrict__ S,
+                                 uint64_t nS, uint32_t stride, uint64_t sr, uint64_t ss, ShjTables t,
+                                 unsigned long long *acc) {
+    __shared__ uint64_t red[64];
+    Acc a;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nR + nS;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const bool isr = i < nR;
+        const uint64_t k = isr ? i : i - nR;
+        const uint64_t w = (isr ? R : S)[k * stride + (stride - 1)];
+        const uint32_t b = (uint32_t)(k / (isr ? sr : ss));
+        if (isr) {
+            if (b) shj_probe(t, 1, w, b - 1, true, a);
         } else {
-            uint64_t *tab = t.tab[own] + ((uint64_t)shj_part(key, t.log2parts) << lo);
-            uint64_t slot = npo_hash(key, lo);
-            for (uint64_t tries = 0;; tries++) {
-                const unsigned long long prev = atomicCAS(reinterpret_cast<unsigned long long *>(tab + slot),
-                                                          (unsigned long long)kEmpty, (unsigned long long)w);
-                if (prev == kEmpty) break;
-                slot = (slot + 1) & mown;
-                if (tries > mown) { atomicExch(err, 2); break; }
-            }
-        }
-        // (2)/(4): probe the other side's table
-        const uint64_t *tab = t.tab[oth] + ((uint64_t)shj_part(key, t.log2parts) << lt);
-        uint64_t slot = npo_hash(key, lt);
-        for (uint64_t tries = 0; tries <= moth; tries++) {
-            const uint64_t v = tab[slot];
-            if (v == kEmpty) break;
-            if (tkey(v) == key) {
-                a.count++;
-                a.sum += side == 0 ? pair_hash(key, tpay(w), tpay(v)) : pair_hash(key, tpay(v), tpay(w));
-            }
-            slot = (slot + 1) & moth;
-        }
-        if (key == 0xFFFFFFFFu && nsent_oth) {
-            a.count += nsent_oth;
-            a.sum += nsent_oth * (side == 0 ? pair_hash(key, tpay(w), 0xFFFFFFFFu) : pair_hash(key, 0xFFFFFFFFu, tpay(w)));
+            shj_probe(t, 0, w, b, false, a);
         }
     }
     block_flush(a, acc, red);
@@ -203,8 +258,8 @@ static EagerPlan plan_eager(Family fam, int model, int nthreads, int group_size,
 
 static size_t eager_plan_bytes(const EagerPlan &p) {
     if (p.fam == Family::Shj)
-        return Workspace::need(1ULL << (p.log2sub[0] + p.log2parts), 8) +
-               Workspace::need(1ULL << (p.log2sub[1] + p.log2parts), 8) + Workspace::need(2, 8);
+        return Workspace::need(1ULL << (p.log2sub[0] + p.log2parts), 16) +
+               Workspace::need(1ULL << (p.log2sub[1] + p.log2parts), 16);
     return 2 * Workspace::need(p.capR + 1, 8) + 2 * Workspace::need(p.capS + 1, 8) +
            2 * Workspace::need(p.run_cap + 1, 8);
 }
@@ -213,11 +268,10 @@ static void take_window(Context *ctx, const EagerPlan &p, EagerWindow &w) {
     if (p.fam == Family::Shj) {
         for (int s = 0; s < 2; s++) {
             w.tab_slots[s] = 1ULL << (p.log2sub[s] + p.log2parts);
-            w.t.tab[s] = ctx->ws.take<uint64_t>(w.tab_slots[s]);
+            w.t.tab[s] = ctx->ws.take<ulonglong2>(w.tab_slots[s]);
             w.t.log2sub[s] = p.log2sub[s];
         }
         w.t.log2parts = p.log2parts;
-        w.t.sent = ctx->ws.take<unsigned long long>(2);
     } else {
         for (int s = 0; s < 2; s++) {
             const uint64_t cap = s ? p.capS : p.capR;
@@ -231,8 +285,7 @@ static void take_window(Context *ctx, const EagerPlan &p, EagerWindow &w) {
 
 static int reset_window(Context *ctx, const EagerPlan &p, EagerWindow &w) {
     if (p.fam == Family::Shj) {
-        for (int s = 0; s < 2; s++) ADB_CK(cudaMemsetAsync(w.t.tab[s], 0xFF, w.tab_slots[s] * 8, ctx->stream));
-        ADB_CK(cudaMemsetAsync(w.t.sent, 0, 16, ctx->stream));
+        for (int s = 0; s < 2; s++) ADB_CK(cudaMemsetAsync(w.t.tab[s], 0xFF, w.tab_slots[s] * 16, ctx->stream));
     } else {
         w.n_accum[0] = w.n_accum[1] = 0;
         w.cur[0] = w.cur[1] = 0;
@@ -246,17 +299,17 @@ static int grid_for(Context *ctx, uint64_t n) {
     return (int)(b < 1 ? 1 : (b > cap ? cap : b));
 }
 
-// SHJ: one micro-batch of each side, R first (shj() alternates R then S).
+// SHJ: micro-batch k of each side, R first (shj() alternates R then S).
 static int shj_step(Context *ctx, EagerWindow &w, const uint64_t *R, uint64_t nr, const uint64_t *S, uint64_t ns,
-                    uint32_t stride, unsigned long long *acc) {
+                    uint32_t stride, uint32_t k, unsigned long long *acc) {
     cudaStream_t st = ctx->stream;
     int *err = reinterpret_cast<int *>(acc + 2);
     if (nr) {
-        shj_batch<<<grid_for(ctx, nr), 256, 0, st>>>(R, stride, nr, 0, w.t, acc, err);
+        shj_batch<<<grid_for(ctx, nr), 256, 0, st>>>(R, stride, nr, 0, k, w.t, acc, err);
         ctx->kernels++;
     }
     if (ns) {
-        shj_batch<<<grid_for(ctx, ns), 256, 0, st>>>(S, stride, ns, 1, w.t, acc, err);
+        shj_batch<<<grid_for(ctx, ns), 256, 0, st>>>(S, stride, ns, 1, k, w.t, acc, err);
         ctx->kernels++;
     }
     ADB_CK(cudaGetLastError());
@@ -312,9 +365,28 @@ static int pmj_step(Context *ctx, EagerWindow &w, const uint64_t *R, uint64_t nr
 }
 
 static int eager_step(Context *ctx, const EagerPlan &p, EagerWindow &w, const uint64_t *R, uint64_t nr,
-                      const uint64_t *S, uint64_t ns, uint32_t stride, unsigned long long *acc) {
-    return p.fam == Family::Shj ? shj_step(ctx, w, R, nr, S, ns, stride, acc)
+                      const uint64_t *S, uint64_t ns, uint32_t stride, uint32_t k, unsigned long long *acc) {
+    return p.fam == Family::Shj ? shj_step(ctx, w, R, nr, S, ns, stride, k, acc)
                                 : pmj_step(ctx, w, R, nr, S, ns, stride, acc);
+}
+
+// Throughput form of one whole window: SHJ in two launches (insert all, probe
+// all with the arrival rule, micro-batches of sr / ss tuples), PMJ as one run.
+static int eager_window_throughput(Context *ctx, const EagerPlan &p, EagerWindow &w, const uint64_t *R, uint64_t nr,
+                                   const uint64_t *S, uint64_t ns, uint32_t stride, uint64_t sr, uint64_t ss,
+                                   unsigned long long *acc) {
+    if (p.fam != Family::Shj) return pmj_step(ctx, w, R, nr, S, ns, stride, acc);
+    if (!nr && !ns) return ADB_OK;
+    cudaStream_t st = ctx->stream;
+    int *err = reinterpret_cast<int *>(acc + 2);
+    const int grid = grid_for(ctx, nr + ns);
+    sr = std::max<uint64_t>(1, sr);
+    ss = std::max<uint64_t>(1, ss);
+    shj_insert_window<<<grid, 256, 0, st>>>(R, nr, S, ns, stride, sr, ss, w.t, err);
+    shj_probe_window<<<grid, 256, 0, st>>>(R, nr, S, ns, stride, sr, ss, w.t, acc);
+    ctx->kernels += 2;
+    ADB_CK(cudaGetLastError());
+    return ADB_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -351,11 +423,13 @@ int run_eager(Context *ctx, const DevJoin &j, Family fam, int model, uint64_t ba
     ADB_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
     ADB_CK(cudaEventRecord(ctx->ev[2], ctx->stream));
     ADB_CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+    if (fam == Family::Shj)   // arrival order = micro-batch order; no real-time release
+        return eager_window_throughput(ctx, p, w, j.R, j.nR, j.S, j.nS, 1, sr, ss, acc);
     for (uint64_t k = 0; k < runs; k++) {
         // the last step takes the left-over of both sides (localjoiner.cpp:575-590)
         const uint64_t r0 = std::min(j.nR, k * sr), r1 = k + 1 == runs ? j.nR : std::min(j.nR, (k + 1) * sr);
         const uint64_t s0 = std::min(j.nS, k * ss), s1 = k + 1 == runs ? j.nS : std::min(j.nS, (k + 1) * ss);
-        ADB_TRY(eager_step(ctx, p, w, j.R + r0, r1 - r0, j.S + s0, s1 - s0, 1, acc));
+        ADB_TRY(eager_step(ctx, p, w, j.R + r0, r1 - r0, j.S + s0, s1 - s0, 1, (uint32_t)k, acc));
     }
     return ADB_OK;
 }
@@ -490,7 +564,12 @@ int stream_join(Context *ctx, Family fam, int model, const adb_stream_tuple *R, 
         uint64_t sr, ss;
         const uint64_t steps = step_sizes(w, &sr, &ss);
         const bool stamp = progress && w < max_windows;
-        for (uint64_t k = 0; k < steps; k++) {
+        if (!realtime && !stamp) {
+            // throughput configuration: the whole window at once (same matches)
+            ADB_CK(cudaEventRecord(ctx->ev[4], st));
+            ADB_TRY(eager_window_throughput(ctx, plan, win, dR + 2 * r0, r1 - r0, dS + 2 * s0, s1 - s0, 2, sr, ss, acc));
+        }
+        for (uint64_t k = 0; (realtime || stamp) && k < steps; k++) {
             const uint64_t a0 = std::min(r1, r0 + k * sr), a1 = k + 1 == steps ? r1 : std::min(r1, r0 + (k + 1) * sr);
             const uint64_t c0 = std::min(s1, s0 + k * ss), c1 = k + 1 == steps ? s1 : std::min(s1, s0 + (k + 1) * ss);
             if (realtime) {
@@ -503,7 +582,7 @@ int stream_join(Context *ctx, Family fam, int model, const adb_stream_tuple *R, 
             }
             if (k + 1 == steps) ADB_CK(cudaEventRecord(ctx->ev[4], st));
             if (stamp) stamp_kernel<<<1, 1, 0, st>>>(nullptr, stamps + 3 * k);
-            ADB_TRY(eager_step(ctx, plan, win, dR + 2 * a0, a1 - a0, dS + 2 * c0, c1 - c0, 2, acc));
+            ADB_TRY(eager_step(ctx, plan, win, dR + 2 * a0, a1 - a0, dS + 2 * c0, c1 - c0, 2, (uint32_t)k, acc));
             if (stamp) {
                 stamp_kernel<<<1, 1, 0, st>>>(acc, stamps + 3 * k + 1);
                 ctx->kernels += 2;

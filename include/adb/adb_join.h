@@ -249,6 +249,23 @@ int adb_serve_run(const adb_serve_config *cfg, const adb_serve_request *req, uin
                   adb_serve_result *res, adb_serve_stats *stats);
 
 /* ---------------------------------------------------------------------- */
+/* One join over several GPUs (one process per GPU).                      */
+/* ---------------------------------------------------------------------- */
+
+/* The split step of a sharded join (no counterpart in the reference, which
+ * runs on one machine): groups the device relation dIn[0..n) by destination
+ * rank into dOut (device, n tuples): the tuples of part p (p < parts <= 32)
+ * are dOut[off_p .. off_p + counts[p]), off_p = counts[0] + .. + counts[p-1],
+ * in no particular order; counts is a host array of `parts` entries.  The
+ * destination of a key is (key * 0x9E3779B1 mod 2^32) * parts / 2^32.  After an
+ * all-to-all of the parts, every rank holds all tuples of its keys from both
+ * relations and joins them alone; the ranks' (count, checksum) pairs add up
+ * (mod 2^64) to the join of the whole relations.  Synchronises `stream`
+ * (NULL = the library stream) before it returns the counts. */
+int adb_shard_split(const adb_tuple *dIn, uint64_t n, uint32_t parts, adb_tuple *dOut, uint64_t *counts,
+                    void *stream);
+
+/* ---------------------------------------------------------------------- */
 /* Device memory helpers for callers without a CUDA runtime of their own. */
 /* ---------------------------------------------------------------------- */
 int adb_device_alloc(void **ptr, size_t bytes);

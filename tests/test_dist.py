@@ -85,3 +85,69 @@ def test_two_ranks_gloo_combine_equals_single():
     for rank, tot, tmax in got:
         assert tot == (want_c, want_k)
         assert tmax == 2.0
+
+
+def _split_np(T, parts):
+    """The split of adb_shard_split, restated with numpy on the CPU."""
+    import torch
+    from alliancedb_b200.dist import shard_of
+    w = T.numpy().view(np.uint64)
+    dst = shard_of(w >> np.uint64(32), parts)
+    order = np.argsort(dst, kind="stable")
+    counts = np.bincount(dst, minlength=parts)
+    return torch.from_numpy(w[order].view(np.int64).copy()), [int(c) for c in counts]
+
+
+def _sharded_worker(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    import datetime
+    import torch
+    import torch.distributed as dist
+    import alliancedb_b200 as adb
+    from alliancedb_b200.dist import shard, shard_of, sharded_join_with
+    from tests.oracle_bind import Oracle
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        o = Oracle()
+        R = adb.gen_uniform(30011, 9000, 71).view(np.int64)
+        S = adb.gen_uniform(25013, 9000, 72).view(np.int64)
+        rl, rh = shard(len(R), rank, world)
+        sl, sh = shard(len(S), rank, world)
+        seen = []
+
+        def join(Rr, Sr):
+            Rw, Sw = Rr.numpy().view(np.uint64), Sr.numpy().view(np.uint64)
+            seen.append((len(Rw), len(Sw), bool((shard_of(Rw >> np.uint64(32), world) == rank).all() and
+                                                (shard_of(Sw >> np.uint64(32), world) == rank).all())))
+            return o.truth(Rw, Sw)
+
+        tot = sharded_join_with(torch.from_numpy(R[rl:rh].copy()), torch.from_numpy(S[sl:sh].copy()), _split_np,
+                                join)
+        q.put((rank, tot, *seen[0]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_join_two_ranks_equals_single_join(oracle):
+    """One join over two gloo ranks: split by destination, all-to-all, local
+    joins (the oracle stands in for the device), all-reduce -- equals the join
+    of the whole relations on both ranks, and every tuple reaches exactly the
+    rank its key is bound for."""
+    import alliancedb_b200 as adb
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_sharded_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    R = adb.gen_uniform(30011, 9000, 71)
+    S = adb.gen_uniform(25013, 9000, 72)
+    want = oracle.truth(R, S)
+    assert all(r[1] == want for r in res)
+    assert sum(r[2] for r in res) == len(R) and sum(r[3] for r in res) == len(S)
+    assert all(r[4] for r in res)
