@@ -13,10 +13,10 @@
 //      keys meet in one partition, as the reference's range partition
 //      guarantees for its key ranges;
 //   2. smj_items, a persistent work-stealing kernel: per work item it copies an
-//      R chunk (<= 8192 tuples) into shared memory with bulk async copies, sorts
+//      R chunk (<= 4096 tuples) into shared memory with bulk async copies, sorts
 //      it, loads and sorts the item's S block, and merge-joins the two sorted
 //      runs with merge-path partitioning across the CTA's threads.
-// The per-chunk sort is an MSD counting sort on the (at most) 12 highest key
+// The per-chunk sort is an MSD counting sort on the (at most) 11 highest key
 // bits that differ within the chunk, followed by an insertion sort inside
 // each bucket: the bits above those are equal across the chunk, so the result
 // is fully sorted by key.  Ties between equal keys stay in arbitrary order,
@@ -28,18 +28,19 @@
 
 namespace adb {
 
-constexpr uint32_t kSmjCap = 8192;                  // tuples per R chunk and per S block
+constexpr uint32_t kSmjCap = 4096;                  // tuples per R chunk and per S block
 constexpr uint32_t kSmjChunkW = kSmjCap - kPageTuples;
-constexpr uint32_t kSmjSPages = kSmjCap / kPageTuples;   // 128 pages <= 8192 tuples
-constexpr uint32_t kSmjMaxPages = 272;              // weight floor 32: <= 8192 / 32 + 1 pages per chunk
-constexpr uint32_t kSmjThreads = 1024;
+constexpr uint32_t kSmjSPages = kSmjCap / kPageTuples;   // 64 pages <= 4096 tuples
+constexpr uint32_t kSmjMaxPages = kSmjCap / kMinPageW + 16;   // pages of one R chunk (weight floor 32)
+constexpr uint32_t kSmjThreads = 512;
+constexpr int kSmjBlocks = 2;                       // CTAs per SM: one's barriers and copies hide behind the other
 
 // A | B | C tuple buffers, bucket counters, two page tables (R pages then S
 // pages: page id, dst << 8 | count), barrier, scratch and two item records.
 constexpr uint32_t kSmjTabEntries = kSmjMaxPages + kSmjSPages + 1;
 constexpr size_t kSmjSmem = (size_t)kSmjCap * 8 * 3 + (size_t)kDualCntWords * 4 + (size_t)kSmjTabEntries * 4 * 2 * 2 +
                             1024;
-static_assert(kSmjSmem <= 232448, "smj_items exceeds the 227 KB shared-memory limit");
+static_assert(kSmjBlocks * (kSmjSmem + 1024) <= 233472, "smj_items CTAs exceed the SM's shared memory");
 static_assert(((size_t)kDualCntWords + (size_t)kSmjTabEntries * 4) % 2 == 0, "mbarrier must be 8-byte aligned");
 
 struct SmjArgs {
@@ -72,7 +73,7 @@ struct SmjRec {
 // Items are pipelined as in radix_join_items: while item i is merge-joined by
 // warps 0 .. 30, the last warp builds the page table of item i + 1 and takes
 // item i + 2, so no dependent global load sits between two items.
-__global__ void __launch_bounds__(kSmjThreads, 1)
+__global__ void __launch_bounds__(kSmjThreads, kSmjBlocks)
 smj_items(SmjArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint64_t *A = reinterpret_cast<uint64_t *>(smem);
@@ -281,7 +282,7 @@ static void smj_bits(uint64_t nR, int part_fanout, uint32_t *b1, uint32_t *b2) {
     if (part_fanout > 1) {
         bits = (int)ceil_log2_u64((uint64_t)part_fanout);
     } else {
-        bits = (int)ceil_log2_u64((nR + 4095) / 4096);   // R partitions of about half a chunk
+        bits = (int)ceil_log2_u64((nR + kSmjCap / 2 - 1) / (kSmjCap / 2));   // R partitions of about half a chunk
     }
     if (bits < 1) bits = 1;
     if (bits > 16) bits = 16;
@@ -340,7 +341,7 @@ int run_smj(Context *ctx, const DevJoin &j, int part_fanout, bool /*multipass*/,
     a.waits_run_out = j.test_flags & ADB_TEST_WAITS_RUN_OUT;
     a.F = F;
     a.mat = j.mat; a.mat_n = acc + 3; a.mat_cap = j.mat_cap;
-    smj_items<<<ctx->num_sms, kSmjThreads, kSmjSmem, st>>>(a);
+    smj_items<<<ctx->num_sms * kSmjBlocks, kSmjThreads, kSmjSmem, st>>>(a);
     ADB_CK(cudaGetLastError());
     ctx->kernels += 4;
     return ADB_OK;

@@ -128,9 +128,9 @@ __device__ __forceinline__ void chunk_sort(const uint64_t *src, uint32_t n, uint
 }
 
 
-constexpr uint32_t kDualBucketBits = 12;
+constexpr uint32_t kDualBucketBits = 11;
 
-// Shared-memory words of dual_chunk_sort's counters: two sides of 2^12 + 1
+// Shared-memory words of dual_chunk_sort's counters: two sides of 2^11 + 1
 // 16-bit counters each, packed two per 32-bit word.
 constexpr uint32_t kDualCntWords = ((1u << kDualBucketBits) + 2);
 
@@ -172,7 +172,7 @@ __device__ __forceinline__ uint32_t inc16(uint32_t *w, uint32_t d) {
 // ex[d] / ey[d] is the end of bucket d of Xo / Yo (unless bitonic).  red holds
 // 96 scratch words.
 //
-// The buckets are the (at most) 12 highest key bits that differ within the two
+// The buckets are the (at most) 11 highest key bits that differ within the two
 // chunks.  When no lower key bit differs, every bucket holds one key value and
 // needs no further order (ties stay in arbitrary order, which merge_join does
 // not depend on), except for payload order among key 0xFFFFFFFF tuples.

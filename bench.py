@@ -25,7 +25,9 @@ the reference's own code compiled from its sources (oracle/_ref) when present,
 otherwise the oracle's CPU restatement, using the host's threads.
 
 Multi-GPU (`--gpus N` under torchrun): every rank joins its own R/S pair of the
-same size (independent windows, no exchange): weak scaling.
+same size (independent windows, no exchange): weak scaling.  With `--shard`
+the ranks run ONE join together (split by key hash, one all-to-all per
+relation, local joins, one all-reduce): strong scaling.
 """
 from __future__ import annotations
 
@@ -263,6 +265,91 @@ def workload_config(args):
                    if (16 << args.log2n) > 126e6 else "inputs smaller than L2")}
 
 
+def shard_main(args):
+    """--shard: ONE join of |R| = |S| = 2^log2n sharded over the ranks (strong
+    scaling): rank r holds slice r of each relation, splits it by key hash
+    (adb_shard_split), one NCCL all-to-all per relation moves the parts, every
+    rank joins what it received, one all-reduce adds (count, checksum).  The
+    timed step is all of that; value = 2^(log2n+1) / max-over-ranks step time."""
+    import datetime
+    import socket
+    import torch
+    import torch.distributed as dist
+    import alliancedb_b200 as adb
+    from alliancedb_b200.dist import max_over_ranks, shard, sharded_join
+
+    if "WORLD_SIZE" not in os.environ:   # plain `python bench.py --shard`: a one-rank group
+        s = socket.socket()
+        s.bind(("127.0.0.1", 0))
+        os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(s.getsockname()[1]), RANK="0", WORLD_SIZE="1",
+                          LOCAL_RANK="0")
+        s.close()
+    world, rank = int(os.environ["WORLD_SIZE"]), int(os.environ["RANK"])
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    try:
+        n = 1 << args.log2n
+        R, S, idx = make_inputs(adb, n, args.theta, 1)   # the same relations on every rank
+        lo, hi = shard(n, rank, world)
+        hR = torch.from_numpy(R.view(np.int64)[lo:hi].copy()).pin_memory()
+        hS = torch.from_numpy(S.view(np.int64)[lo:hi].copy()).pin_memory()
+        dR, dS = hR.to(dev), hS.to(dev)
+        stream = torch.cuda.current_stream(dev)
+
+        def barrier():
+            dist.barrier()
+            torch.cuda.synchronize(dev)
+
+        for _ in range(args.warmup):
+            got = sharded_join(args.algo, dR, dS)
+        if rank == 0:
+            closed = fk_closed_form(R, S, idx)
+            if got != closed:
+                raise AssertionError(f"sharded join {got} != closed form {closed}")
+        del idx
+        barrier()
+        with ClockSampler(local) as clk:
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                assert sharded_join(args.algo, dR, dS) == got
+            e1.record(stream)
+            barrier()
+        ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dev)
+        # end to end: this rank's slice from pinned host memory each step
+        e_ms = []
+        for _ in range(max(1, args.steps // 2)):
+            barrier()
+            a = time.perf_counter()
+            assert sharded_join(args.algo, hR.to(dev, non_blocking=True), hS.to(dev, non_blocking=True)) == got
+            torch.cuda.synchronize(dev)
+            e_ms.append((time.perf_counter() - a) * 1e3)
+        e2e_ms = max_over_ranks(statistics.median(e_ms), dev)
+        hbm, peak_kind = peaks()
+        pipe_gbs = ALG_BYTES.get(args.algo, 24) * 2 * n / (ms / 1e3) / 1e9 / world
+        line = {"metric": "join input tuples/s", "value": 2 * n / (ms / 1e3), "unit": "tuples/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "u32 key/payload (integer)", "data": "synthetic",
+                "config": {**workload_config(args),
+                           "sharding": f"one join over {world} GPU(s): split by key hash, one NCCL all-to-all per "
+                                       "relation, local joins, one all-reduce of (count, checksum)"},
+                "e2e": {"value": 2 * n / (e2e_ms / 1e3), "unit": "tuples/s", "h2d_bytes_per_step": 16 * n,
+                        "d2h_bytes_per_step": 32 * world, "ms_per_step": e2e_ms},
+                "roofline": {"bound": "hbm", "kernel": "whole sharded pipeline, per GPU", "achieved": pipe_gbs,
+                             "peak": hbm, "unit": "GB/s", "frac": pipe_gbs / hbm, "peak_source": peak_kind,
+                             "traffic": None},
+                "clocks": clk.summary(),
+                "result": {"count": got[0], "checksum": hex(got[1]),
+                           "verified": "equal to the closed form of the foreign-key workload"}}
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+    finally:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -277,6 +364,8 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=120.0,
                     help="--impl reference: stop timing once this many seconds of calls have run")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--shard", action="store_true",
+                    help="one join sharded over the ranks (strong scaling) instead of one join per rank")
     ap.add_argument("--no-forms", action="store_true",
                     help="skip the batched / served / stream sub-objects of the default line")
     ap.add_argument("--workload", default="join", choices=["join", "batch", "serve", "stream"],
@@ -298,6 +387,9 @@ def main():
                 "stream": workloads.bench_stream}[args.workload](args)
         print(json.dumps(line), flush=True)
         return
+
+    if args.shard:
+        return shard_main(args)
 
     import torch
     import alliancedb_b200 as adb

@@ -31,8 +31,9 @@ def test_split_parts_hold_their_keys(parts, n):
     d_in = torch.from_numpy(w.view(np.int64).copy()).to(dev)
     d_out = torch.empty_like(d_in)
     counts = (C.c_uint64 * parts)()
+    stream = torch.cuda.current_stream(dev).cuda_stream   # the stream that wrote d_in
     st = adb.lib().adb_shard_split(d_in.data_ptr() if n else None, n, parts, d_out.data_ptr() if n else None, counts,
-                                   None)
+                                   stream)
     assert st == 0, adb.lib().adb_last_error().decode()
     out = d_out.cpu().numpy().view(np.uint64)
     dst = shard_of(w >> np.uint64(32), parts)
