@@ -108,10 +108,10 @@ __host__ __device__ __forceinline__ uint32_t unit_pages_for(uint64_t pages1_both
 }
 
 // Shared memory of one pass:
-//   stage[kPTile] u64 | inbuf[kPTile] u64 | cnt[2][F] | toff[F] | lim[2][F] | b1[2][F] | b2[2][F]
-//   | npos[F] u32 | misc[48] u32 | paged input only: upage[kMaxUnitPages] u32 | ucnt[kMaxUnitPages] u8
+//   stage[kPTile] u64 | cnt[2][F] | toff[F] | lim[F] | b1[F] | b2[F] | npos[F] u32 | misc[48] u32
+//   | paged input only: upage[kMaxUnitPages] u32 | ucnt[kMaxUnitPages] u8
 __host__ __device__ __forceinline__ size_t pass_smem(uint32_t F, bool paged) {
-    return (size_t)kPTile * 8 * 2 + (size_t)F * 4 * 10 + 48 * 4 + (paged ? (size_t)kMaxUnitPages * 5 : 0);
+    return (size_t)kPTile * 8 + (size_t)F * 4 * 7 + 48 * 4 + (paged ? (size_t)kMaxUnitPages * 5 : 0);
 }
 
 __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x, int lane) {
@@ -123,57 +123,33 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x, int lane) {
     return x;
 }
 
-// Warps that compute a tile's digit runs (step B): one per 128 digits.
-__host__ __device__ __forceinline__ uint32_t pass_b_warps(uint32_t F) { return F > 128 ? (F + 127) / 128 : 1u; }
-
-// Asynchronous global -> shared copies of one thread (cp.async, completion by
-// cp.async.wait_group of the same thread); src_bytes < 16 zero-fills the rest.
-__device__ __forceinline__ void cp_async16(void *sdst, const void *gsrc, uint32_t src_bytes) {
-    const uint32_t d = (uint32_t)__cvta_generic_to_shared(sdst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(gsrc), "r"(src_bytes) : "memory");
-}
-__device__ __forceinline__ void cp_async8(void *sdst, const void *gsrc) {
-    const uint32_t d = (uint32_t)__cvta_generic_to_shared(sdst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-
 // One pass over one input unit (a flat chunk, a unit of input pages, or a
 // unit of a segment).  Per tile of up to kPTile tuples:
-//   L  every thread copies its own slots of the tile from global memory into
-//      the input buffer (cp.async, 16 bytes at a time), one tile ahead;
-//   A  every thread reads its slots back and ranks its tuples within their
-//      digit (shared atomics on cnt[tile parity][d]);
-//   B  the B warps (one per 128 digits, up to four digits per lane) turn the
-//      counts into the tile's digit runs (toff), take the pages each digit's
-//      stream needs from the CTA's pool, and advance the streams (npos = next
-//      free slot of the digit's current page, kNone when there is none);
-//      lim / b1 / b2 of the tile's parity say where its stage slots go: slot i
-//      of digit d goes to i + b1[d] while i < lim[d] (the rest of the current
-//      page), else to i + b2[d] (the pages taken in B, consecutive in the pool);
+//   A  every thread ranks its tuples within their digit (shared atomics on
+//      cnt[tile parity][d]);
+//   B  warp 0 (up to 128 digits, F / 32 per lane) or warps 0 .. F/32 - 1 (one
+//      digit per lane) turn the counts into the tile's digit runs (toff), take
+//      the pages each digit's stream needs from the CTA's pool, and advance
+//      the streams (npos = next free slot of the digit's current page, kNone
+//      when there is none);
 //   C  every thread puts its tuples into the stage, grouped by digit;
-//   D  threads copy stage slots to their pages, two adjacent slots with one
-//      16-byte store when their destinations are adjacent and 16-byte aligned;
-//      the thread that writes a page's first slot also writes the page's log
-//      entry.
-// The steps are pipelined over tiles: while the B warps compute tile t's runs,
-// the other warps scatter tile t - 1 (its lim, b1, b2 and size sit in the other
-// parity; the stage is free again before C of tile t), and every thread's
-// copies of tile t + 1 are in flight from the start of the iteration until A
-// of tile t + 1 at its end.  A tile costs two block barriers; no warp waits on
-// the run computation.  Consecutive stage slots of a digit go to consecutive
-// addresses, so warps store contiguous runs; a run's partial first and last
-// 32-byte sectors are completed by the neighbouring tiles of the same stream
-// while the line is still in L2.  kMode: 0 flat input, 1 paged input (pass 2),
-// 2 segmented flat input (batched windows).
+//   D  every thread copies stage slots to their pages: slot i of digit d goes
+//      to i + b1[d] while i < lim[d] (the rest of the current page), else to
+//      i + b2[d] (the pages taken in B, consecutive in the pool); the thread
+//      that writes a page's first slot also writes the page's log entry.
+// Consecutive stage slots of a digit go to consecutive addresses, so warps
+// store contiguous runs; a run's partial first and last 32-byte sectors are
+// completed by the neighbouring tiles of the same stream while the line is
+// still in L2.  Three barriers per tile (four above 128 digits); the next
+// tile's loads are in flight during D.  kMode: 0 flat input, 1 paged input
+// (pass 2), 2 segmented flat input (batched windows).
 template <int kMode, int kThreads>
 __global__ void __launch_bounds__(kThreads, kPassMinBlocks)
 partition_pass(PassArgs a) {
     constexpr bool kPaged = kMode == 1;
     constexpr int kPer = kPTile / kThreads;
     static_assert(kPer % 2 == 0 && kThreads % 32 == 0 && (kPTile / kPageTuples) % (kThreads / 32) == 0, "tile shape");
-    static_assert((1u << kMaxPassBits) <= 4u * 128u && kThreads / 32 > 4, "step B: at most four B warps, one left for D");
+    static_assert((1u << kMaxPassBits) <= (uint32_t)kThreads, "one digit per thread in step B");
     extern __shared__ __align__(16) unsigned char smem[];
     const int relidx = blockIdx.y, g = blockIdx.x;
     const PassIn &in = relidx ? a.in[1] : a.in[0];
@@ -203,26 +179,23 @@ partition_pass(PassArgs a) {
         }
     }
     const uint32_t F = df.mask + 1;
-    uint64_t *stage = reinterpret_cast<uint64_t *>(smem);              // [kPTile]
-    uint64_t *inbuf = stage + kPTile;                                   // [kPTile]
-    uint32_t *cnt = reinterpret_cast<uint32_t *>(inbuf + kPTile);       // [2][F]
+    uint64_t *stage = reinterpret_cast<uint64_t *>(smem);
+    uint32_t *cnt = reinterpret_cast<uint32_t *>(stage + kPTile);   // [2][F]
     uint32_t *toff = cnt + 2 * F;
-    uint32_t *lim = toff + F;           // [2][F]
-    uint32_t *b1 = lim + 2 * F;         // [2][F]
-    uint32_t *b2 = b1 + 2 * F;          // [2][F]
-    uint32_t *npos = b2 + 2 * F;
-    uint32_t *misc = npos + F;          // [0] pool pages taken, [2 + parity] stage slots of the tile,
-                                        // [8..12) per-B-warp totals of the digit scan
+    uint32_t *lim = toff + F;
+    uint32_t *b1 = lim + F;
+    uint32_t *b2 = b1 + F;
+    uint32_t *npos = b2 + F;
+    uint32_t *misc = npos + F;          // [0] pool pages taken, [1] tuples in the tile,
+                                        // [8..24) per-warp totals of the digit scan
     uint32_t *upage = misc + 48;        // paged input: this unit's pages
     uint8_t *ucnt = reinterpret_cast<uint8_t *>(upage + kMaxUnitPages);
 
     const PageSet &o = relidx ? a.out[1] : a.out[0];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, lane = tid & 31;
     const uint32_t pool_base = kMode == 2 ? in.unit_pool[g] : (uint32_t)g * a.pool_cap;
     const uint32_t pool_cap = kMode == 2 ? in.unit_pool[g + 1] - pool_base : a.pool_cap;
     const uint32_t dbase = kMode == 2 ? in.seg_dbase[p1] : p1 * F;   // output digit = dbase + d
-    const uint32_t nbw = pass_b_warps(F);                             // B warps
-    const uint32_t q = (F + 32 * nbw - 1) / (32 * nbw);               // digits per B lane (<= 4)
 
     for (uint32_t d = tid; d < F; d += kThreads) {
         cnt[d] = 0;
@@ -241,40 +214,53 @@ partition_pass(PassArgs a) {
     // ---- tiles: kPTile flat tuples, or kPTile / 64 input pages
     constexpr uint64_t kStep = kPaged ? (uint64_t)(kPTile / kPageTuples) : (uint64_t)kPTile;
     const bool vec = !kPaged && ((reinterpret_cast<uintptr_t>(in.in + b) & 15) == 0);
-    // Slots of this thread: pair k = input-buffer slots s(k), s(k) + 1 with
-    //   flat input:  s = 2 (k kThreads + tid), tuples t0 + s, t0 + s + 1;
-    //   paged input: s = 64 pg + 2 (tid % 32), pg = k (kThreads / 32) + tid / 32,
-    //                the tile's pg-th page, its slots 2 (tid % 32), + 1.
-    auto pair_slot = [&](int k) -> uint32_t {
-        return kPaged ? ((uint32_t)k * (kThreads / 32) + (uint32_t)(tid / 32)) * kPageTuples + 2u * (uint32_t)lane
-                      : 2u * ((uint32_t)k * kThreads + (uint32_t)tid);
-    };
-    auto pair_count = [&](uint64_t t0, int k) -> uint32_t {   // tuples of pair k present (0, 1, 2)
+    uint64_t w[kPer];
+    uint32_t valid = 0;   // bit k: w[k] holds a tuple
+    auto load_tile = [&](uint64_t t0) {
+        valid = 0;
         if (kPaged) {
-            const uint64_t li = t0 + (uint64_t)k * (kThreads / 32) + tid / 32;
-            const uint32_t c = li < e ? ucnt[li - b] : 0u, s2 = 2u * (uint32_t)lane;
-            return c > s2 + 1 ? 2u : (c > s2 ? 1u : 0u);
-        }
-        const uint64_t i = t0 + pair_slot(k);
-        return i + 1 < e ? 2u : (i < e ? 1u : 0u);
-    };
-    // L. this thread's copies of the tile at t0 into its input-buffer slots
-    auto copy_tile = [&](uint64_t t0) {
+            // tuple pair k of this thread: slots 2 (tid % 32), +1 of the tile's page k * (kThreads / 32) + tid / 32
+            const uint32_t slot = 2 * (tid & 31);
 #pragma unroll
-        for (int k = 0; k < kPer / 2; k++) {
-            const uint32_t n = pair_count(t0, k), s = pair_slot(k);
-            if (!n) continue;
-            const uint64_t *src = kPaged ? in.pages + (uint64_t)upage[t0 + (uint64_t)k * (kThreads / 32) + tid / 32 - b] *
-                                                          kPageTuples + 2u * (uint32_t)lane
-                                         : in.in + t0 + s;
-            if (kPaged || vec) {
-                cp_async16(inbuf + s, src, n * 8);
-            } else {   // relation not 16-byte aligned: 8-byte copies
-                cp_async8(inbuf + s, src);
-                if (n == 2) cp_async8(inbuf + s + 1, src + 1);
+            for (int k = 0; k < kPer / 2; k++) {
+                const uint64_t li = t0 + (uint64_t)k * (kThreads / 32) + tid / 32;
+                const uint32_t c = li < e ? ucnt[li - b] : 0u;
+                if (slot + 1 < c) {
+                    const ulonglong2 v = __ldcs(reinterpret_cast<const ulonglong2 *>(
+                        in.pages + (uint64_t)upage[li - b] * kPageTuples + slot));
+                    w[2 * k] = v.x;
+                    w[2 * k + 1] = v.y;
+                    valid |= 3u << (2 * k);
+                } else {
+                    const bool ok = slot < c;
+                    w[2 * k] = ok ? ld_stream(in.pages + (uint64_t)upage[li - b] * kPageTuples + slot) : 0;
+                    w[2 * k + 1] = 0;
+                    valid |= (ok ? 1u : 0u) << (2 * k);
+                }
+            }
+        } else if (vec) {
+#pragma unroll
+            for (int k = 0; k < kPer / 2; k++) {
+                const uint64_t i = t0 + 2 * ((uint64_t)k * kThreads + tid);
+                if (i + 1 < e) {
+                    const ulonglong2 v = __ldcs(reinterpret_cast<const ulonglong2 *>(in.in + i));
+                    w[2 * k] = v.x;
+                    w[2 * k + 1] = v.y;
+                    valid |= 3u << (2 * k);
+                } else {
+                    w[2 * k] = i < e ? ld_stream(in.in + i) : 0;
+                    w[2 * k + 1] = 0;
+                    valid |= (i < e ? 1u : 0u) << (2 * k);
+                }
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < kPer; k++) {
+                const uint64_t i = t0 + (uint64_t)k * kThreads + tid;
+                w[k] = i < e ? ld_stream(in.in + i) : 0;
+                valid |= (i < e ? 1u : 0u) << k;
             }
         }
-        cp_async_commit();
     };
 
     // L2 prefetch of a whole flat tile (one bulk prefetch; paged input is not
@@ -288,171 +274,147 @@ partition_pass(PassArgs a) {
         }
     };
 
-    // A. read this thread's slots of the tile at t0 (after its copies landed)
-    //    and rank each tuple within its digit (counters of parity par)
-    uint64_t w[kPer];
-    uint32_t valid = 0;      // bit k: w[k] holds a tuple
-    uint32_t rk[kPer / 2];   // two 16-bit ranks per word
-    auto rank_tile = [&](uint64_t t0, uint32_t par) {
-        cp_async_wait_all();
-        valid = 0;
-#pragma unroll
-        for (int k = 0; k < kPer / 2; k++) {
-            const uint32_t n = pair_count(t0, k);
-            const ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(inbuf + pair_slot(k));
-            w[2 * k] = v.x;
-            w[2 * k + 1] = v.y;
-            valid |= ((n >= 1 ? 1u : 0u) | (n == 2 ? 2u : 0u)) << (2 * k);
-        }
-        uint32_t *c = cnt + par * F;
+    if (b < e) {
+        prefetch_tile(b + kStep);
+        load_tile(b);
+    }
+    uint32_t par = 0;
+    for (uint64_t t0 = b; t0 < e; t0 += kStep, par ^= F) {
+        uint32_t *c = cnt + par;
+        // A. rank each tuple within its digit
+        uint32_t rk[kPer / 2];   // two 16-bit ranks per word
 #pragma unroll
         for (int k = 0; k < kPer; k++) {
             const uint32_t r = (valid >> k) & 1 ? atomicAdd(&c[df(tkey(w[k]))], 1u) : 0u;
             if (k & 1) rk[k / 2] |= r << 16; else rk[k / 2] = r;
         }
-    };
-
-    // B. digit runs of the tile of parity par, its pages and stream positions
-    //    (B warps only; lane l of B warp bw owns digits (bw * 32 + l) * q ..
-    //    + q - 1; the B warps' totals are combined through misc and a named
-    //    barrier).  New pages get their log entry in D, from the thread that
-    //    writes their first slot.
-    auto run_tile = [&](uint32_t par) {
-        uint32_t *c = cnt + par * F;
-        uint32_t *lm = lim + par * F, *p1b = b1 + par * F, *p2b = b2 + par * F;
+        __syncthreads();
+        // B. digit runs of the tile, pages, stream positions.  Up to 128 digits
+        //    warp 0 alone (lane l: digits l*q .. l*q + q - 1, q = F / 32), above
+        //    that warp w < F / 32 takes digits 32w .. 32w + 31, one per lane, and
+        //    the warps' totals are combined through shared memory (one extra
+        //    barrier).  New pages get their log entry in D, from the thread that
+        //    writes their first slot.
+        auto run_digit = [&](uint32_t d, uint32_t L, uint32_t p, uint32_t off, uint32_t first) {
+            const uint32_t room = p == kNone ? 0u : kPageTuples - (p & (kPageTuples - 1));
+            c[d] = 0;
+            toff[d] = off;
+            lim[d] = off + (L < room ? L : room);
+            b1[d] = p - off;
+            uint32_t np = p + L;
+            if (L > room) {
+                const uint32_t need = (L - room + kPageTuples - 1) / kPageTuples;
+                if (first + need > pool_cap) {   // cannot happen: the pool covers the input
+                    atomicExch(a.err, 3);
+                    first = pool_cap - need;
+                }
+                const uint32_t nx = (pool_base + first) * kPageTuples - room;
+                b2[d] = nx - off;
+                np = nx + L;
+            }
+            if (L && (np & (kPageTuples - 1)) == 0) np = kNone;   // page exactly full
+            npos[d] = np;
+        };
         auto pages_for = [&](uint32_t L, uint32_t p) {
             const uint32_t room = p == kNone ? 0u : kPageTuples - (p & (kPageTuples - 1));
             return L > room ? (L - room + kPageTuples - 1) / kPageTuples : 0u;
         };
-        constexpr int kQ = 4;
-        uint32_t Ls[kQ], Ps[kQ], sumL = 0, sumN = 0;
+        if (F <= 128) {
+            constexpr int kQ = 4;
+            const uint32_t q = (F + 31) / 32;
+            if (tid < 32) {
+                uint32_t Ls[kQ], Ps[kQ], sumL = 0, sumN = 0;
 #pragma unroll
-        for (int j = 0; j < kQ; j++) {
-            const uint32_t d = ((uint32_t)warp * 32 + lane) * q + j;
-            Ls[j] = 0;
-            Ps[j] = kNone;
-            if ((uint32_t)j < q && d < F) {
-                Ls[j] = c[d];
-                Ps[j] = npos[d];
-                sumL += Ls[j];
-                sumN += pages_for(Ls[j], Ps[j]);
-            }
-        }
-        const uint32_t v = sumL | (sumN << 16);   // L <= kPTile per tile, pages < 2^16
-        const uint32_t inc = warp_incl_scan(v, lane);
-        const uint32_t pool0 = misc[0];
-        uint32_t before = 0, all = __shfl_sync(0xffffffffu, inc, 31);
-        if (nbw > 1) {
-            if (lane == 31) misc[8 + warp] = inc;
-            asm volatile("bar.sync 1, %0;" ::"r"(nbw * 32) : "memory");   // B warps only
-            all = 0;
-            for (uint32_t k = 0; k < nbw; k++) {
-                const uint32_t tv = misc[8 + k];
-                if (k < (uint32_t)warp) before += tv;
-                all += tv;
-            }
-        }
-        uint32_t off = (before + inc - v) & 0xFFFFu, first = pool0 + ((before + inc - v) >> 16);
-#pragma unroll
-        for (int j = 0; j < kQ; j++) {
-            const uint32_t d = ((uint32_t)warp * 32 + lane) * q + j;
-            if ((uint32_t)j < q && d < F) {
-                const uint32_t L = Ls[j], p = Ps[j];
-                const uint32_t room = p == kNone ? 0u : kPageTuples - (p & (kPageTuples - 1));
-                c[d] = 0;
-                toff[d] = off;
-                lm[d] = off + (L < room ? L : room);
-                p1b[d] = p - off;
-                uint32_t np = p + L;
-                if (L > room) {
-                    const uint32_t need = (L - room + kPageTuples - 1) / kPageTuples;
-                    uint32_t f = first;
-                    if (f + need > pool_cap) {   // cannot happen: the pool covers the input
-                        atomicExch(a.err, 3);
-                        f = pool_cap - need;
+                for (int j = 0; j < kQ; j++) {
+                    const uint32_t d = (uint32_t)lane * q + j;
+                    Ls[j] = 0;
+                    Ps[j] = kNone;
+                    if ((uint32_t)j < q && d < F) {
+                        Ls[j] = c[d];
+                        Ps[j] = npos[d];
+                        sumL += Ls[j];
+                        sumN += pages_for(Ls[j], Ps[j]);
                     }
-                    const uint32_t nx = (pool_base + f) * kPageTuples - room;
-                    p2b[d] = nx - off;
-                    np = nx + L;
-                    first += need;
                 }
-                if (L && (np & (kPageTuples - 1)) == 0) np = kNone;   // page exactly full
-                npos[d] = np;
-                off += L;
+                const uint32_t v = sumL | (sumN << 16);   // L <= kPTile, pages < 2^16
+                const uint32_t inc = warp_incl_scan(v, lane);
+                const uint32_t all = __shfl_sync(0xffffffffu, inc, 31);
+                const uint32_t pool0 = misc[0];
+                uint32_t off = (inc - v) & 0xFFFFu, first = pool0 + ((inc - v) >> 16);
+#pragma unroll
+                for (int j = 0; j < kQ; j++) {
+                    const uint32_t d = (uint32_t)lane * q + j;
+                    if ((uint32_t)j < q && d < F) {
+                        run_digit(d, Ls[j], Ps[j], off, first);
+                        off += Ls[j];
+                        first += pages_for(Ls[j], Ps[j]);
+                    }
+                }
+                __syncwarp();
+                if (lane == 0) {
+                    misc[0] = pool0 + (all >> 16);
+                    misc[1] = all & 0xFFFFu;
+                }
+            }
+        } else {
+            const uint32_t nbw = (F + 31) / 32;                 // B warps
+            const int bw = tid >> 5;
+            const uint32_t d = (uint32_t)tid;                   // this lane's digit
+            uint32_t L = 0, p = kNone, need = 0, inc = 0, pool0 = 0;
+            if (bw < (int)nbw) {
+                if (d < F) {
+                    L = c[d];
+                    p = npos[d];
+                    need = pages_for(L, p);
+                }
+                inc = warp_incl_scan(L | (need << 16), lane);   // L <= kPTile, pages of 32 digits < 2^16
+                pool0 = misc[0];
+                if (lane == 31) misc[8 + bw] = inc;
+            }
+            __syncthreads();   // every B warp has read misc[0] and written its total
+            if (bw < (int)nbw) {
+                // totals of the warps before this one, and of all of them
+                uint32_t before_t = 0, before_p = 0, all_t = 0, all_p = 0;
+                for (uint32_t k = 0; k < nbw; k++) {
+                    const uint32_t tv = misc[8 + k];
+                    if ((int)k < bw) { before_t += tv & 0xFFFFu; before_p += tv >> 16; }
+                    all_t += tv & 0xFFFFu;
+                    all_p += tv >> 16;
+                }
+                const uint32_t ex = inc - (L | (need << 16));
+                if (d < F) run_digit(d, L, p, before_t + (ex & 0xFFFFu), pool0 + before_p + (ex >> 16));
+                if (bw == 0 && lane == 0) {   // warp 0 read misc[0] before the shuffle above
+                    misc[0] = pool0 + all_p;
+                    misc[1] = all_t;
+                }
             }
         }
-        if (nbw > 1) asm volatile("bar.sync 1, %0;" ::"r"(nbw * 32) : "memory");   // every B warp read misc
-        if (warp == 0 && lane == 0) {
-            misc[0] = pool0 + (all >> 16);
-            misc[2 + par] = all & 0xFFFFu;
-        }
-    };
-
-    // C. stage the register tuples grouped by digit
-    auto stage_tile = [&]() {
+        __syncthreads();
+        // C. stage the tile grouped by digit
 #pragma unroll
         for (int k = 0; k < kPer; k++)
             if ((valid >> k) & 1)
                 stage[toff[df(tkey(w[k]))] + ((rk[k / 2] >> ((k & 1) * 16)) & 0xFFFFu)] = w[k];
-    };
-
-    // D. stage slots to their pages (lim, b1, b2, size of parity par), by
-    //    threads t .. t + nt - 1
-    auto scatter_tile = [&](uint32_t par, uint32_t t, uint32_t nt) {
-        const uint32_t *lm = lim + par * F, *p1b = b1 + par * F, *p2b = b2 + par * F;
-        const uint32_t n = misc[2 + par];
-        auto dest = [&](uint32_t i, uint64_t v, uint32_t &d) {
-            d = df(tkey(v));
-            return i + (i < lm[d] ? p1b[d] : p2b[d]);
-        };
-        auto page_head = [&](uint32_t dst, uint32_t d) {
+        const uint32_t tile_n = misc[1];
+        if (t0 + kStep < e) {   // in flight during D; the tile after that into L2
+            prefetch_tile(t0 + 2 * kStep);
+            load_tile(t0 + kStep);
+        }
+        __syncthreads();
+        // D. stage slots to their pages
+        for (uint32_t i = tid; i < tile_n; i += kThreads) {
+            const uint64_t v = stage[i];
+            const uint32_t d = df(tkey(v));
+            const uint32_t dst = i + (i < lim[d] ? b1[d] : b2[d]);
+            o.pages[dst] = v;
             if ((dst & (kPageTuples - 1)) == 0) {   // first slot of a page taken in B
                 o.log[dst / kPageTuples] = dbase + d;
                 o.pcount[dst / kPageTuples] = kPageTuples;
             }
-        };
-        for (uint32_t i = 2 * t; i < n; i += 2 * nt) {
-            // slot i + 1 may be stale when i + 1 == n (n < kPTile then): not used
-            const ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(stage + i);
-            uint32_t d0, d1 = 0;
-            const uint32_t x0 = dest(i, v.x, d0);
-            if (i + 1 < n) {
-                const uint32_t x1 = dest(i + 1, v.y, d1);
-                if (x1 == x0 + 1 && (x0 & 1) == 0) {
-                    *reinterpret_cast<ulonglong2 *>(o.pages + x0) = v;
-                } else {
-                    o.pages[x0] = v.x;
-                    o.pages[x1] = v.y;
-                }
-                page_head(x1, d1);
-            } else {
-                o.pages[x0] = v.x;
-            }
-            page_head(x0, d0);
         }
-    };
-
-    if (b < e) {
-        copy_tile(b);
-        prefetch_tile(b + kStep);
-        rank_tile(b, 0);
+        // the next tile's A uses the other counter array and registers only;
+        // its B / C run after the next barrier, when every thread is past D
     }
-    __syncthreads();
-    uint32_t par = 0;
-    for (uint64_t t0 = b; t0 < e; t0 += kStep, par ^= 1) {
-        const bool more = t0 + kStep < e;
-        if (more) {   // the next tile's copies: in flight until its ranks at the end of this iteration
-            copy_tile(t0 + kStep);
-            prefetch_tile(t0 + 2 * kStep);
-        }
-        if ((uint32_t)warp < nbw) run_tile(par);
-        else if (t0 != b) scatter_tile(par ^ 1, tid - nbw * 32, kThreads - nbw * 32);
-        __syncthreads();   // runs of this tile known; the previous tile scattered
-        stage_tile();
-        if (more) rank_tile(t0 + kStep, par ^ 1);
-        __syncthreads();   // this tile staged; the next tile ranked
-    }
-    if (b < e) scatter_tile(par ^ 1, tid, kThreads);   // the last tile
     __syncthreads();
     // E. fill of each digit's last page
     for (uint32_t d = tid; d < F; d += kThreads) {

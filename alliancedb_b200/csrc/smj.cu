@@ -82,8 +82,8 @@ smj_items(SmjArgs a) {
     uint32_t *cnt = reinterpret_cast<uint32_t *>(C + kSmjCap);
     uint32_t *ptab = cnt + kDualCntWords;                    // [2] x {pg[kSmjTabEntries], dst << 8 | count []}
     uint64_t *bar = reinterpret_cast<uint64_t *>(ptab + 4 * kSmjTabEntries);
-    uint64_t *red = bar + 2;                                 // 64 u64 (96 u32 of sort scratch)
-    SmjRec *rec = reinterpret_cast<SmjRec *>(red + 64);      // [2]
+    uint64_t *red = bar + 2;                                 // 96 u64 (192 u32 of sort scratch)
+    SmjRec *rec = reinterpret_cast<SmjRec *>(red + 96);      // [2]
 
     const uint32_t n_items = *a.n_items;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -206,7 +206,8 @@ smj_items(SmjArgs a) {
         // sorted R (+ pads) in B, sorted S (+ pads) in A; the pads are the last
         // words of each run and a real all-ones tuple is the same word, so
         // dropping as many words as there are pads is exact
-        const DualSort ds = dual_chunk_sort(A, rslots, B, C, sslots, A, cnt, reinterpret_cast<uint32_t *>(red));
+        const DualSort ds =
+            dual_chunk_sort(A, rslots, B, C, sslots, A, cnt, reinterpret_cast<uint32_t *>(red), spad);
         const uint32_t nr = rslots - rpad, ns = sslots - spad;
         const uint64_t *Rs = B, *Ss = A;
 
@@ -228,9 +229,28 @@ smj_items(SmjArgs a) {
             }
         };
         // all-ones words beyond the pads: real tuples with key 0xFFFFFFFF
-        const bool ones = !ds.bitonic && (rslots - (ds.nb ? ds.ex[ds.nb - 1] : 0u) != rpad ||
-                                          sslots - (ds.nb ? ds.ey[ds.nb - 1] : 0u) != spad);
-        if (!ds.bitonic && !ds.max_key && !ones) {
+        const bool ones = !ds.y_single && !ds.bitonic && (rslots - (ds.nb ? ds.ex[ds.nb - 1] : 0u) != rpad ||
+                                                          sslots - (ds.nb ? ds.ey[ds.nb - 1] : 0u) != spad);
+        if (ds.y_single) {
+            // the S block is one key K (a hot key under skew), left unsorted in C
+            // with its pads: every S word but the pads meets the run of K in the
+            // key-sorted R chunk (R pads sort last; K < 0xFFFFFFFF)
+            const uint32_t K = ds.y_key;
+            uint32_t lo = 0, hi = rslots;   // first R slot with key >= K
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (tkey(Rs[mid]) < K) lo = mid + 1; else hi = mid;
+            }
+            uint32_t e = lo;
+            while (e < rslots && tkey(Rs[e]) == K) e++;
+            for (uint32_t j = threadIdx.x; j < sslots && warp != kCtl && e > lo; j += kWork) {
+                const uint64_t s = C[j];
+                if (s == ~0ULL) continue;   // a pad
+                uint64_t sh = 0;
+                bool have = false;
+                for (uint32_t t = lo; t < e; t++) emit(s, Rs[t], sh, have);
+            }
+        } else if (!ds.bitonic && !ds.max_key && !ones) {
             // both runs are ordered by the same buckets: S bucket d meets R bucket
             // d, whose sorted range [ex[d - 1], ex[d]) holds every R tuple that
             // can have the S tuple's key; no key is 0xFFFFFFFF, so no pad matches

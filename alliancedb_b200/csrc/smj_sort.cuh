@@ -152,6 +152,9 @@ struct DualSort {
     uint32_t shift, bmask, nb;   // bucket(v) = v == ~0 ? nb : (key >> shift) & bmask
     bool bitonic;                // a side took the bitonic path: bucket ends are not valid
     bool max_key;                // a word other than all-ones has key 0xFFFFFFFF
+    bool y_single;               // every Y word but its ypads all-ones pads has key y_key
+                                 // (< 0xFFFFFFFF): Y is left unsorted in place, ey is not set
+    uint32_t y_key;
     const uint16_t *ex, *ey;     // end of bucket d of Xo / Yo: ex[d], ey[d] (unless bitonic)
     __device__ __forceinline__ uint32_t bucket(uint64_t v) const {
         return v == ~0ULL ? nb : (tkey(v) >> shift) & bmask;
@@ -170,23 +173,34 @@ __device__ __forceinline__ uint32_t inc16(uint32_t *w, uint32_t d) {
 // the barriers of two calls.  Yo may be X's buffer (X is consumed first); Xo, X
 // and Y must be distinct.  cnt holds kDualCntWords words: afterwards the result's
 // ex[d] / ey[d] is the end of bucket d of Xo / Yo (unless bitonic).  red holds
-// 96 scratch words.
+// 192 scratch words.  ypads = all-ones pad words among Y's.
+//
+// A Y chunk of one key (a hot key's block under skew: every increment would hit
+// one shared counter) is not sorted at all: y_single reports it, and the caller
+// pairs its words with X's run of that key.
 //
 // The buckets are the (at most) 11 highest key bits that differ within the two
 // chunks.  When no lower key bit differs, every bucket holds one key value and
 // needs no further order (ties stay in arbitrary order, which merge_join does
 // not depend on), except for payload order among key 0xFFFFFFFF tuples.
 __device__ __forceinline__ DualSort dual_chunk_sort(const uint64_t *X, uint32_t nx, uint64_t *Xo, const uint64_t *Y,
-                                                    uint32_t ny, uint64_t *Yo, uint32_t *cnt, uint32_t *red) {
+                                                    uint32_t ny, uint64_t *Yo, uint32_t *cnt, uint32_t *red,
+                                                    uint32_t ypads) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int nw = (int)(blockDim.x >> 5);
-    uint32_t a = 0xFFFFFFFFu, o = 0, mk = 0;
+    uint32_t a = 0xFFFFFFFFu, o = 0, mk = 0, ay = 0xFFFFFFFFu, oy = 0, onesy = 0;
     for (uint32_t i = threadIdx.x; i < nx + ny; i += blockDim.x) {
         const uint64_t v = i < nx ? X[i] : Y[i - nx];
         if (v != ~0ULL) {
             a &= tkey(v);
             o |= tkey(v);
             mk |= tkey(v) == 0xFFFFFFFFu;
+            if (i >= nx) {
+                ay &= tkey(v);
+                oy |= tkey(v);
+            }
+        } else if (i >= nx) {
+            onesy++;
         }
     }
 #pragma unroll
@@ -194,20 +208,36 @@ __device__ __forceinline__ DualSort dual_chunk_sort(const uint64_t *X, uint32_t 
         a &= __shfl_xor_sync(0xffffffffu, a, s);
         o |= __shfl_xor_sync(0xffffffffu, o, s);
         mk |= __shfl_xor_sync(0xffffffffu, mk, s);
+        ay &= __shfl_xor_sync(0xffffffffu, ay, s);
+        oy |= __shfl_xor_sync(0xffffffffu, oy, s);
+        onesy += __shfl_xor_sync(0xffffffffu, onesy, s);
     }
-    if (lane == 0) { red[wid] = a; red[32 + wid] = o; red[64 + wid] = mk; }
+    if (lane == 0) {
+        red[wid] = a; red[32 + wid] = o; red[64 + wid] = mk;
+        red[96 + wid] = ay; red[128 + wid] = oy; red[160 + wid] = onesy;
+    }
     for (uint32_t d = threadIdx.x; d < kDualCntWords; d += blockDim.x) cnt[d] = 0;
     __syncthreads();
     a = lane < nw ? red[lane] : 0xFFFFFFFFu;
     o = lane < nw ? red[32 + lane] : 0u;
     mk = lane < nw ? red[64 + lane] : 0u;
+    ay = lane < nw ? red[96 + lane] : 0xFFFFFFFFu;
+    oy = lane < nw ? red[128 + lane] : 0u;
+    onesy = lane < nw ? red[160 + lane] : 0u;
 #pragma unroll
     for (int s = 16; s > 0; s >>= 1) {
         a &= __shfl_xor_sync(0xffffffffu, a, s);
         o |= __shfl_xor_sync(0xffffffffu, o, s);
         mk |= __shfl_xor_sync(0xffffffffu, mk, s);
+        ay &= __shfl_xor_sync(0xffffffffu, ay, s);
+        oy |= __shfl_xor_sync(0xffffffffu, oy, s);
+        onesy += __shfl_xor_sync(0xffffffffu, onesy, s);
     }
     DualSort r;
+    // Y of one key: ay == oy over its non-pad words, none of them all-ones
+    // beyond the pads (so no real key-0xFFFFFFFF tuple hides among the pads)
+    r.y_single = ny > onesy && ay == oy && ay != 0xFFFFFFFFu && onesy == ypads;
+    r.y_key = ay;
     const uint32_t vary = (a & ~o) ? 0u : a ^ o;
     const uint32_t hi = vary ? 31 - __clz(vary) : 0u;
     const uint32_t nbits = vary == 0 ? 0u : (hi + 1 < kDualBucketBits ? hi + 1 : kDualBucketBits);
@@ -220,7 +250,8 @@ __device__ __forceinline__ DualSort dual_chunk_sort(const uint64_t *X, uint32_t 
     uint16_t *cx = reinterpret_cast<uint16_t *>(wx), *cy = reinterpret_cast<uint16_t *>(wy);
     r.ex = cx;
     r.ey = cy;
-    for (uint32_t i = threadIdx.x; i < nx + ny; i += blockDim.x) {
+    const uint32_t nyc = r.y_single ? 0u : ny;   // Y words counted and placed
+    for (uint32_t i = threadIdx.x; i < nx + nyc; i += blockDim.x) {
         if (i < nx) inc16(wx, r.bucket(X[i]));
         else inc16(wy, r.bucket(Y[i - nx]));
     }
@@ -246,7 +277,7 @@ __device__ __forceinline__ DualSort dual_chunk_sort(const uint64_t *X, uint32_t 
         Xo[inc16(wx, r.bucket(v))] = v;
     }
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < ny; i += blockDim.x) {
+    for (uint32_t i = threadIdx.x; i < nyc; i += blockDim.x) {
         const uint64_t v = Y[i];
         Yo[inc16(wy, r.bucket(v))] = v;
     }

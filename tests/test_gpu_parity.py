@@ -178,3 +178,33 @@ def test_threads_share_device_context(oracle):
     for t in th:
         t.join()
     assert got == want
+
+
+@pytest.mark.parametrize("algo", ["m-way", "m-pass", "m-way+skew", "PRO", "NPO"])
+def test_single_key_probe_blocks(oracle, algo):
+    """S blocks of one key (a hot key under skew: the sort-merge join leaves such
+    a block unsorted and pairs it with R's run of that key), next to blocks with
+    a few other keys; R holds the hot key once and another key many times."""
+    rng = np.random.default_rng(17)
+    rk = rng.permutation(np.arange(1, 20001, dtype=np.uint32))
+    rk[:600] = 777                                           # a key repeated 600 times in R
+    R = adb.tuples(rk)
+    sk = np.full(40000, 4242, np.uint32)                     # the hot key (once in R)
+    sk[::997] = rng.integers(1, 20001, size=len(sk[::997]), dtype=np.uint32)
+    sk[20000:26000] = 777                                    # a block of the repeated key
+    S = adb.tuples(sk)
+    check(oracle, algo, R, S)
+
+
+@pytest.mark.parametrize("algo", ["m-way", "m-way+skew"])
+def test_single_key_block_with_all_ones_tuples(oracle, algo):
+    """An S block of one key plus real all-ones tuples (key and payload
+    0xFFFFFFFF, the pad word's value): they must join R's key-0xFFFFFFFF tuples."""
+    R = adb.tuples(np.array([5, 0xFFFFFFFF, 9, 0xFFFFFFFF], np.uint32),
+                   np.array([1, 0xFFFFFFFF, 3, 7], np.uint32))
+    sk = np.full(3000, 5, np.uint32)
+    sp = np.arange(3000, dtype=np.uint32)
+    sk[[10, 2000]] = 0xFFFFFFFF
+    sp[[10, 2000]] = 0xFFFFFFFF
+    S = adb.tuples(sk, sp)
+    check(oracle, algo, R, S)
