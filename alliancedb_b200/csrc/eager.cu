@@ -176,7 +176,8 @@ static uint32_t shj_log2parts(int model, int nthreads, int group_size) {
 
 static uint32_t shj_log2sub(uint64_t n, uint32_t log2parts) {
     // two slots per tuple in each sub-table, with slack for an uneven key split
-    const uint64_t per = (n >> log2parts) + (n >> (log2parts + 1)) + 64;
+    // when the table is split
+    const uint64_t per = (n >> log2parts) + (log2parts ? (n >> (log2parts + 1)) : 0) + 64;
     uint32_t l = ceil_log2_u64(2 * per);
     return l < 4 ? 4 : l;
 }
@@ -559,6 +560,7 @@ int stream_join(Context *ctx, Family fam, int model, const adb_stream_tuple *R, 
     const auto wall0 = std::chrono::steady_clock::now();
     for (uint64_t w = 0; w < nwin; w++) {
         const uint64_t r0 = rb[w], r1 = rb[w + 1], s0 = sb[w], s1 = sb[w + 1];
+        ADB_CK(cudaEventRecord(ctx->ev[4], st));   // throughput form: the window's device time from here
         ADB_TRY(reset_window(ctx, plan, win));
         ADB_CK(cudaMemsetAsync(acc, 0, 32, st));
         uint64_t sr, ss;
@@ -566,7 +568,6 @@ int stream_join(Context *ctx, Family fam, int model, const adb_stream_tuple *R, 
         const bool stamp = progress && w < max_windows;
         if (!realtime && !stamp) {
             // throughput configuration: the whole window at once (same matches)
-            ADB_CK(cudaEventRecord(ctx->ev[4], st));
             ADB_TRY(eager_window_throughput(ctx, plan, win, dR + 2 * r0, r1 - r0, dS + 2 * s0, s1 - s0, 2, sr, ss, acc));
         }
         for (uint64_t k = 0; (realtime || stamp) && k < steps; k++) {

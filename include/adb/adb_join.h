@@ -142,7 +142,10 @@ typedef struct adb_window_result {
     uint64_t window_start_ms;
     uint64_t n_r, n_s;
     uint64_t count, checksum;
-    float latency_ms;           /* close-of-window -> result on host, device clock */
+    float latency_ms;           /* realtime: close of the window -> result on the host (wall clock);
+                                   per-batch form: the last batch -> result (device clock);
+                                   throughput form: the window's whole device time (table
+                                   reset, joins, result copy) */
     float reserved;
 } adb_window_result;
 
