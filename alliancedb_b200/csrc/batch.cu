@@ -203,19 +203,29 @@ int batch_launch(Context *ctx, const uint64_t *dR, const uint64_t *r_off, const 
                          Workspace::need(pages * kPageTuples / kChunkW + Dt + 1, 8) + Workspace::need(2 * W + 8, 8);
     ADB_TRY(ctx->ws.reserve(bytes + 8192));
 
+    // the plan (window bits, partition bases, unit offsets, segments, unit pools):
+    // laid out in the pinned staging buffer exactly as in the workspace, one copy
+    const size_t plan_off = ctx->ws.off;
     uint8_t *d_bits = ctx->ws.take<uint8_t>(W);
     uint32_t *d_wbase = ctx->ws.take<uint32_t>(W + 1);
     uint32_t *d_uoff[2] = {ctx->ws.take<uint32_t>(W + 1), ctx->ws.take<uint32_t>(W + 1)};
     uint64_t *d_seg[2] = {ctx->ws.take<uint64_t>(W + 1), ctx->ws.take<uint64_t>(W + 1)};
-    ADB_CK(cudaMemcpyAsync(d_bits, bits.data(), W, cudaMemcpyHostToDevice, st));
-    ADB_CK(cudaMemcpyAsync(d_wbase, wbase.data(), (W + 1) * 4, cudaMemcpyHostToDevice, st));
-    ADB_CK(cudaMemcpyAsync(d_uoff[0], uoffR.data(), (W + 1) * 4, cudaMemcpyHostToDevice, st));
-    ADB_CK(cudaMemcpyAsync(d_uoff[1], uoffS.data(), (W + 1) * 4, cudaMemcpyHostToDevice, st));
-    ADB_CK(cudaMemcpyAsync(d_seg[0], segR.data(), (W + 1) * 8, cudaMemcpyHostToDevice, st));
-    ADB_CK(cudaMemcpyAsync(d_seg[1], segS.data(), (W + 1) * 8, cudaMemcpyHostToDevice, st));
     uint32_t *d_upool[2] = {ctx->ws.take<uint32_t>(G + 1), ctx->ws.take<uint32_t>(G + 1)};
-    ADB_CK(cudaMemcpyAsync(d_upool[0], upool[0].data(), (G + 1) * 4, cudaMemcpyHostToDevice, st));
-    ADB_CK(cudaMemcpyAsync(d_upool[1], upool[1].data(), (G + 1) * 4, cudaMemcpyHostToDevice, st));
+    const size_t plan_bytes = ctx->ws.off - plan_off;
+    ADB_TRY(pinned_reserve(&ctx->h_stage, &ctx->h_stage_cap, plan_bytes));   // the last plan's copy is done
+    char *h = ctx->h_stage;
+    auto put = [&](const void *dev_at, const void *src, size_t n) {
+        memcpy(h + (reinterpret_cast<const char *>(dev_at) - (ctx->ws.base + plan_off)), src, n);
+    };
+    put(d_bits, bits.data(), W);
+    put(d_wbase, wbase.data(), (W + 1) * 4);
+    put(d_uoff[0], uoffR.data(), (W + 1) * 4);
+    put(d_uoff[1], uoffS.data(), (W + 1) * 4);
+    put(d_seg[0], segR.data(), (W + 1) * 8);
+    put(d_seg[1], segS.data(), (W + 1) * 8);
+    put(d_upool[0], upool[0].data(), (G + 1) * 4);
+    put(d_upool[1], upool[1].data(), (G + 1) * 4);
+    ADB_CK(cudaMemcpyAsync(ctx->ws.base + plan_off, h, plan_bytes, cudaMemcpyHostToDevice, st));
 
     PassArgs a{};
     for (int r = 0; r < 2; r++) {
@@ -304,8 +314,8 @@ int batch_launch(Context *ctx, const uint64_t *dR, const uint64_t *r_off, const 
 
 static int batch_join_all(Context *ctx, const uint64_t *dR, const uint64_t *r_off, const uint64_t *dS,
                           const uint64_t *s_off, uint32_t W, uint64_t *counts, uint64_t *sums) {
-    unsigned long long *h = nullptr;
-    ADB_CK(cudaMallocHost(&h, (2 * W + 8) * 8));
+    ADB_TRY(pinned_reserve(&ctx->h_out, &ctx->h_out_cap, (2 * (size_t)W + 8) * 8));
+    unsigned long long *h = reinterpret_cast<unsigned long long *>(ctx->h_out);
     int s = batch_launch(ctx, dR, r_off, dS, s_off, W, h);
     if (s == ADB_OK) {
         cudaError_t e = cudaStreamSynchronize(ctx->stream);
@@ -322,7 +332,6 @@ static int batch_join_all(Context *ctx, const uint64_t *dR, const uint64_t *r_of
             }
         }
     }
-    cudaFreeHost(h);
     return s;
 }
 

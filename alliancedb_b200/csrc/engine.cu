@@ -53,6 +53,22 @@ int Workspace::reserve(size_t bytes) {
     return ADB_OK;
 }
 
+int pinned_reserve(char **buf, size_t *cap, size_t bytes) {
+    if (bytes <= *cap) return ADB_OK;
+    if (*buf) cudaFreeHost(*buf);
+    *buf = nullptr;
+    *cap = 0;
+    const size_t want = bytes + (bytes >> 2);
+    if (cudaMallocHost(reinterpret_cast<void **>(buf), want) != cudaSuccess) {
+        cudaGetLastError();
+        *buf = nullptr;
+        set_error("pinned host buffer of %zu bytes", want);
+        return ADB_ERR_OOM;
+    }
+    *cap = want;
+    return ADB_OK;
+}
+
 void Workspace::release() {
     if (base) cudaFree(base);
     base = nullptr;
@@ -113,6 +129,8 @@ void ctx_destroy(Context *c) {
     for (auto &e : c->ev)
         if (e) cudaEventDestroy(e);
     if (c->h_res) cudaFreeHost(c->h_res);
+    if (c->h_stage) cudaFreeHost(c->h_stage);
+    if (c->h_out) cudaFreeHost(c->h_out);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }

@@ -13,6 +13,8 @@
 namespace adb {
 
 void set_error(const char *fmt, ...);
+// Grows the pinned host buffer *buf to at least `bytes` (its old contents are lost).
+int pinned_reserve(char **buf, size_t *cap, size_t bytes);
 
 #define ADB_CK(call)                                                                      \
     do {                                                                                  \
@@ -57,6 +59,13 @@ struct Context {
     cudaEvent_t ev[12] = {};
     Workspace ws;
     unsigned long long *h_res = nullptr;   // pinned: [0] count [1] checksum [2] err [3] mat_n ...
+    // pinned, grow-only host buffers of the batched path: the per-call plan (one
+    // host -> device copy) and the per-window results (one copy back); growing
+    // one needs its previous use finished
+    char *h_stage = nullptr;
+    size_t h_stage_cap = 0;
+    char *h_out = nullptr;
+    size_t h_out_cap = 0;
     bool attrs_set = false;
     int kernels = 0;                       // kernels launched by the current call
     std::recursive_mutex mu;               // held by the call that uses this context
