@@ -62,8 +62,8 @@ KERNELS = {
               3: ("radix_join_items<Chain>", 8, (273641984 + 7539456) / 2**25)},
     "npo": {0: ("npo_build", 8, None), 3: ("npo_probe", 8, None)},
     "smj": {0: ("partition_pass (both passes)", 32,
-                (271129856 + 214481152 + 275816192 + 215750912) / 2**25),
-            3: ("smj_items", 8, (276513536 + 4389632) / 2**25)},
+                (271074048 + 215111680 + 279591680 + 219554048) / 2**25),
+            3: ("smj_items", 8, (281795584 + 3697664) / 2**25)},
 }
 
 
