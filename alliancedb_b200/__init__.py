@@ -251,12 +251,29 @@ def join(algo: str, R: np.ndarray, S: np.ndarray, params: JoinParams | None = No
     return _result(r)
 
 
+CUDA_STREAM_LEGACY = 1   # cudaStreamLegacy, the legacy default stream
+
+
+def stream_handle(stream) -> int | None:
+    """The cudaStream_t to hand the C API for `stream`: None keeps the
+    library's own stream (NULL there, a non-blocking stream that is not ordered
+    with the legacy default stream); a torch.cuda.Stream or a raw handle is
+    passed on, and handle 0, torch's default stream (the legacy NULL stream),
+    becomes cudaStreamLegacy so that the work is ordered with what torch and
+    torch.distributed queue on that stream."""
+    if stream is None:
+        return None
+    h = stream if isinstance(stream, int) else stream.cuda_stream
+    return h or CUDA_STREAM_LEGACY
+
+
 def join_device(algo: str, dR: int, nR: int, dS: int, nS: int, params: JoinParams | None = None,
-                stream: int | None = None) -> Result:
-    """Join device-resident relations (raw device pointers) through adb_join_device."""
+                stream=None) -> Result:
+    """Join device-resident relations (raw device pointers) through
+    adb_join_device, on `stream` (see stream_handle)."""
     r = JoinResult()
     st = lib().adb_join_device(algo.encode(), dR or None, nR, dS or None, nS,
-                               C.byref(params) if params is not None else None, C.byref(r), stream)
+                               C.byref(params) if params is not None else None, C.byref(r), stream_handle(stream))
     _check(st)
     return _result(r)
 

@@ -27,8 +27,17 @@ namespace adb {
 constexpr int kShardThreads = 256;
 constexpr uint32_t kMaxShardParts = 32;
 
+// On the device the high word comes from __umulhi: the widened form
+// ((uint64_t)h * parts) >> 32, used as the index of the shared-memory atomics
+// below, built (nvcc 12.9, sm_100a, ptxas at its default optimisation level)
+// into kernels that counted every key in part 0; the same source was right
+// at -Xptxas -O0 and with __umulhi, a masked index or global atomics.
 __host__ __device__ __forceinline__ uint32_t shard_of(uint32_t key, uint32_t parts) {
+#ifdef __CUDA_ARCH__
+    return __umulhi(key * 0x9E3779B1u, parts);
+#else
     return (uint32_t)(((uint64_t)(key * 0x9E3779B1u) * parts) >> 32);
+#endif
 }
 
 __host__ __device__ __forceinline__ uint64_t shard_chunk(uint64_t n, uint32_t blocks) {

@@ -98,7 +98,7 @@ def sharded_join(algo: str, dR, dS, params=None):
     import torch
     import alliancedb_b200 as adb
     dev = dR.device
-    stream = torch.cuda.current_stream(dev).cuda_stream
+    stream = adb.stream_handle(torch.cuda.current_stream(dev))   # where NCCL's results are ordered
 
     def split(T, parts):
         out = torch.empty_like(T)

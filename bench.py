@@ -106,31 +106,43 @@ class ClockSampler:
         bus = f"{props.pci_domain_id:08x}:{props.pci_bus_id:02x}:{props.pci_device_id:02x}.0"
         return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
 
-    def _run(self):
+    def _run(self, nv, h):
+        try:
+            while not self._stop.is_set():
+                self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM),
+                                     nv.nvmlDeviceGetCurrentClocksEventReasons(h)))
+                self._first.set()
+                self._stop.wait(self.period)
+        except Exception as e:
+            self.error = f"{type(e).__name__}: {e}"
+        self._first.set()
+
+    def __enter__(self):
+        # NVML is set up here, and the first sample taken, before the timed
+        # region starts, so that short regions are sampled too
+        self._first = threading.Event()
+        self.t = None
         try:
             nv, h = self._handle()
             self.bits = self._reasons(nv)
             self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
-            while not self._stop.is_set():
-                self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM),
-                                     nv.nvmlDeviceGetCurrentClocksEventReasons(h)))
-                self._stop.wait(self.period)
         except Exception as e:   # no NVML: the line says so instead of guessing clocks
             self.error = f"{type(e).__name__}: {e}"
-
-    def __enter__(self):
-        self.t = threading.Thread(target=self._run, daemon=True)
+            return self
+        self.t = threading.Thread(target=self._run, args=(nv, h), daemon=True)
         self.t.start()
-        time.sleep(0.02)
+        self._first.wait(timeout=2)
         return self
 
     def __exit__(self, *a):
         self._stop.set()
-        self.t.join(timeout=5)
+        if self.t is not None:
+            self.t.join(timeout=5)
 
     def summary(self):
-        sm = [c for c, _ in self.samples]
-        reasons = sorted({name for _, r in self.samples for name, bit in self.bits.items() if r & bit})
+        run = self.samples[1:] or self.samples   # the first sample precedes the timed region
+        sm = [c for c, _ in run]
+        reasons = sorted({name for _, r in run for name, bit in self.bits.items() if r & bit})
         out = {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz, "reasons": reasons,
                "samples": len(sm), "source": "NVML every 5 ms during the timed region"}
         if self.error:
@@ -315,7 +327,9 @@ def shard_main(args):
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             for _ in range(args.steps):
-                assert sharded_join(args.algo, dR, dS) == got
+                step = sharded_join(args.algo, dR, dS)
+                if step != got:
+                    raise AssertionError(f"sharded join {step} != {got} of the warm-up")
             e1.record(stream)
             barrier()
         ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dev)
@@ -324,7 +338,9 @@ def shard_main(args):
         for _ in range(max(1, args.steps // 2)):
             barrier()
             a = time.perf_counter()
-            assert sharded_join(args.algo, hR.to(dev, non_blocking=True), hS.to(dev, non_blocking=True)) == got
+            step = sharded_join(args.algo, hR.to(dev, non_blocking=True), hS.to(dev, non_blocking=True))
+            if step != got:
+                raise AssertionError(f"sharded join {step} != {got} of the warm-up")
             torch.cuda.synchronize(dev)
             e_ms.append((time.perf_counter() - a) * 1e3)
         e2e_ms = max_over_ranks(statistics.median(e_ms), dev)
@@ -413,7 +429,7 @@ def main():
     hR = torch.from_numpy(R.view(np.int64)).pin_memory()
     hS = torch.from_numpy(S.view(np.int64)).pin_memory()
     stream = torch.cuda.current_stream(dev)
-    sp = stream.cuda_stream
+    sp = adb.stream_handle(stream)   # torch's stream, so the events below bracket the join's kernels
 
     params = adb.default_params(radix_bits=args.radix_bits) if args.radix_bits else None
 

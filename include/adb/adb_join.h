@@ -121,7 +121,10 @@ int adb_join(const char *algo, const adb_tuple *R, uint64_t nR, const adb_tuple 
              const adb_join_params *p, adb_join_result *out);
 
 /* Join two device-resident relations on `stream` (a cudaStream_t, NULL = the
- * library stream).  Returns after the result is on the host. */
+ * library stream).  Returns after the result is on the host.  The library
+ * stream is non-blocking: it is not ordered with the legacy default stream,
+ * so a caller whose inputs are produced there (torch's default stream, an
+ * NCCL receive that torch orders on it) passes cudaStreamLegacy. */
 int adb_join_device(const char *algo, const adb_tuple *dR, uint64_t nR, const adb_tuple *dS,
                     uint64_t nS, const adb_join_params *p, adb_join_result *out, void *stream);
 

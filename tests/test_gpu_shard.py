@@ -31,7 +31,7 @@ def test_split_parts_hold_their_keys(parts, n):
     d_in = torch.from_numpy(w.view(np.int64).copy()).to(dev)
     d_out = torch.empty_like(d_in)
     counts = (C.c_uint64 * parts)()
-    stream = torch.cuda.current_stream(dev).cuda_stream   # the stream that wrote d_in
+    stream = adb.stream_handle(torch.cuda.current_stream(dev))   # the stream that wrote d_in
     st = adb.lib().adb_shard_split(d_in.data_ptr() if n else None, n, parts, d_out.data_ptr() if n else None, counts,
                                    stream)
     assert st == 0, adb.lib().adb_last_error().decode()
