@@ -70,6 +70,8 @@ struct SmjRec {
     uint32_t pad_;
 };
 
+static_assert(16 + 8 * 96 + 2 * sizeof(SmjRec) <= 1024, "barrier, scratch and records exceed the tail");
+
 // Items are pipelined as in radix_join_items: while item i is merge-joined by
 // warps 0 .. 30, the last warp builds the page table of item i + 1 and takes
 // item i + 2, so no dependent global load sits between two items.
@@ -84,6 +86,7 @@ smj_items(SmjArgs a) {
     uint64_t *bar = reinterpret_cast<uint64_t *>(ptab + 4 * kSmjTabEntries);
     uint64_t *red = bar + 2;                                 // 96 u64 (192 u32 of sort scratch)
     SmjRec *rec = reinterpret_cast<SmjRec *>(red + 96);      // [2]
+    __shared__ uint32_t runn;                                // length of R's run of a single S key
 
     const uint32_t n_items = *a.n_items;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -205,9 +208,20 @@ smj_items(SmjArgs a) {
         __syncthreads();
         // sorted R (+ pads) in B, sorted S (+ pads) in A; the pads are the last
         // words of each run and a real all-ones tuple is the same word, so
-        // dropping as many words as there are pads is exact
-        const DualSort ds =
-            dual_chunk_sort(A, rslots, B, C, sslots, A, cnt, reinterpret_cast<uint32_t *>(red), spad);
+        // dropping as many words as there are pads is exact.  An S block of one
+        // key K is not sorted, and neither is R: R's run of K is gathered into B.
+        uint32_t *red32 = reinterpret_cast<uint32_t *>(red);
+        if (threadIdx.x == 0) runn = 0;   // read after the analysis barrier
+        DualSort ds = dual_analyze(A, rslots, C, sslots, cnt, red32, spad);
+        if (ds.y_single) {
+            for (uint32_t i = threadIdx.x; i < rslots; i += blockDim.x) {
+                const uint64_t v = A[i];   // pads are all-ones words: K < 0xFFFFFFFF never meets them
+                if (tkey(v) == ds.y_key) B[atomicAdd(&runn, 1u)] = v;
+            }
+            __syncthreads();
+        } else {
+            dual_sort_rest(ds, A, rslots, B, C, sslots, A, cnt, red32);
+        }
         const uint32_t nr = rslots - rpad, ns = sslots - spad;
         const uint64_t *Rs = B, *Ss = A;
 
@@ -233,22 +247,14 @@ smj_items(SmjArgs a) {
                                                           sslots - (ds.nb ? ds.ey[ds.nb - 1] : 0u) != spad);
         if (ds.y_single) {
             // the S block is one key K (a hot key under skew), left unsorted in C
-            // with its pads: every S word but the pads meets the run of K in the
-            // key-sorted R chunk (R pads sort last; K < 0xFFFFFFFF)
-            const uint32_t K = ds.y_key;
-            uint32_t lo = 0, hi = rslots;   // first R slot with key >= K
-            while (lo < hi) {
-                const uint32_t mid = (lo + hi) >> 1;
-                if (tkey(Rs[mid]) < K) lo = mid + 1; else hi = mid;
-            }
-            uint32_t e = lo;
-            while (e < rslots && tkey(Rs[e]) == K) e++;
-            for (uint32_t j = threadIdx.x; j < sslots && warp != kCtl && e > lo; j += kWork) {
+            // with its pads: every S word but the pads meets R's run of K, B[0..runn)
+            const uint32_t nrun = runn;
+            for (uint32_t j = threadIdx.x; j < sslots && warp != kCtl && nrun; j += kWork) {
                 const uint64_t s = C[j];
                 if (s == ~0ULL) continue;   // a pad
                 uint64_t sh = 0;
                 bool have = false;
-                for (uint32_t t = lo; t < e; t++) emit(s, Rs[t], sh, have);
+                for (uint32_t t = 0; t < nrun; t++) emit(s, Rs[t], sh, have);
             }
         } else if (!ds.bitonic && !ds.max_key && !ones) {
             // both runs are ordered by the same buckets: S bucket d meets R bucket

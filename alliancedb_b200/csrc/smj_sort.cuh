@@ -155,6 +155,7 @@ struct DualSort {
     bool y_single;               // every Y word but its ypads all-ones pads has key y_key
                                  // (< 0xFFFFFFFF): Y is left unsorted in place, ey is not set
     uint32_t y_key;
+    uint32_t all_and, vary;      // AND of all keys; key bits that differ (0: none)
     const uint16_t *ex, *ey;     // end of bucket d of Xo / Yo: ex[d], ey[d] (unless bitonic)
     __device__ __forceinline__ uint32_t bucket(uint64_t v) const {
         return v == ~0ULL ? nb : (tkey(v) >> shift) & bmask;
@@ -168,24 +169,17 @@ __device__ __forceinline__ uint32_t inc16(uint32_t *w, uint32_t d) {
     return (atomicAdd(&w[d >> 1], 1u << sh) >> sh) & 0xFFFFu;
 }
 
-// chunk_sort of two chunks at once with one bucket function: X[0..nx) -> Xo
-// and Y[0..ny) -> Yo (nx, ny <= 8192), in the same order rules, with about half
-// the barriers of two calls.  Yo may be X's buffer (X is consumed first); Xo, X
-// and Y must be distinct.  cnt holds kDualCntWords words: afterwards the result's
-// ex[d] / ey[d] is the end of bucket d of Xo / Yo (unless bitonic).  red holds
-// 192 scratch words.  ypads = all-ones pad words among Y's.
-//
-// A Y chunk of one key (a hot key's block under skew: every increment would hit
-// one shared counter) is not sorted at all: y_single reports it, and the caller
-// pairs its words with X's run of that key.
-//
-// The buckets are the (at most) 11 highest key bits that differ within the two
-// chunks.  When no lower key bit differs, every bucket holds one key value and
-// needs no further order (ties stay in arbitrary order, which merge_join does
-// not depend on), except for payload order among key 0xFFFFFFFF tuples.
-__device__ __forceinline__ DualSort dual_chunk_sort(const uint64_t *X, uint32_t nx, uint64_t *Xo, const uint64_t *Y,
-                                                    uint32_t ny, uint64_t *Yo, uint32_t *cnt, uint32_t *red,
-                                                    uint32_t ypads) {
+// Scratch words of red[] that dual_chunk_sort uses: [0, 192) the analysis,
+// [0, 32) the scan.
+constexpr uint32_t kDualRedWords = 192;
+
+// First half of dual_chunk_sort: the bucket function of X[0..nx) and
+// Y[0..ny) (the (at most) 11 highest key bits that differ within both) and
+// whether Y is a single key.  Also zeroes the counters.  Ends with a barrier
+// after which every thread holds the result; red is still being read (the
+// next barrier frees it).
+__device__ __forceinline__ DualSort dual_analyze(const uint64_t *X, uint32_t nx, const uint64_t *Y, uint32_t ny,
+                                                 uint32_t *cnt, uint32_t *red, uint32_t ypads) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int nw = (int)(blockDim.x >> 5);
     uint32_t a = 0xFFFFFFFFu, o = 0, mk = 0, ay = 0xFFFFFFFFu, oy = 0, onesy = 0;
@@ -245,24 +239,54 @@ __device__ __forceinline__ DualSort dual_chunk_sort(const uint64_t *X, uint32_t 
     r.nb = 1u << nbits;
     r.bmask = r.nb - 1;
     r.max_key = mk != 0;
+    r.all_and = a;
+    r.vary = vary;
+    r.bitonic = false;
+    const uint32_t W = r.nb + 1;
+    r.ex = reinterpret_cast<const uint16_t *>(cnt);
+    r.ey = reinterpret_cast<const uint16_t *>(cnt + (W + 1) / 2);
+    return r;
+}
+
+// Second half of dual_chunk_sort (every thread calls it right after
+// dual_analyze, with the same arguments): counts, one scan of both sides'
+// counters, scatter, then the order inside buckets that hold several keys.
+__device__ __forceinline__ void dual_sort_rest(DualSort &r, const uint64_t *X, uint32_t nx, uint64_t *Xo,
+                                               const uint64_t *Y, uint32_t ny, uint64_t *Yo, uint32_t *cnt,
+                                               uint32_t *red) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nw = (int)(blockDim.x >> 5);
     const uint32_t nb = r.nb, W = nb + 1;   // counters per side; [nb] = all-ones words
     uint32_t *wx = cnt, *wy = cnt + (W + 1) / 2;   // packed counter words of each side
     uint16_t *cx = reinterpret_cast<uint16_t *>(wx), *cy = reinterpret_cast<uint16_t *>(wy);
-    r.ex = cx;
-    r.ey = cy;
     const uint32_t nyc = r.y_single ? 0u : ny;   // Y words counted and placed
     for (uint32_t i = threadIdx.x; i < nx + nyc; i += blockDim.x) {
         if (i < nx) inc16(wx, r.bucket(X[i]));
         else inc16(wy, r.bucket(Y[i - nx]));
     }
     __syncthreads();   // also: every thread has read red
-    {   // exclusive scans of both sides' counters, contiguous counters per thread
+    {   // exclusive scan of both sides' counters, contiguous counters per thread;
+        // every warp scans the warp totals itself, so one barrier suffices
         const uint32_t per = (2 * W + blockDim.x - 1) / blockDim.x;
         const uint32_t d0 = threadIdx.x * per, d1 = min(2 * W, d0 + per);
         uint32_t loc = 0;
         for (uint32_t d = d0; d < d1; d++) loc += d < W ? cx[d] : cy[d - W];
-        uint32_t tot;
-        uint32_t ex = block_exclusive_scan(loc, red, &tot);
+        uint32_t x = loc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) red[wid] = x;
+        __syncthreads();
+        uint32_t t = lane < nw ? red[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        const uint32_t before = __shfl_sync(0xffffffffu, t, wid > 0 ? wid - 1 : 0);   // warps 0 .. wid - 1
+        uint32_t ex = (wid ? before : 0u) + x - loc;
         for (uint32_t d = d0; d < d1; d++) {
             uint16_t &c = d < W ? cx[d] : cy[d - W];
             const uint32_t v = c;
@@ -270,7 +294,7 @@ __device__ __forceinline__ DualSort dual_chunk_sort(const uint64_t *X, uint32_t 
             ex += v;
         }
     }
-    __syncthreads();
+    __syncthreads();   // red[0..32) is not written again before the next analysis
     // X first: Yo may be X's own buffer
     for (uint32_t i = threadIdx.x; i < nx; i += blockDim.x) {
         const uint64_t v = X[i];
@@ -285,14 +309,14 @@ __device__ __forceinline__ DualSort dual_chunk_sort(const uint64_t *X, uint32_t 
     // cx / cy[d] = end of bucket d.  Buckets that need whole-word order: all of
     // them when lower key bits vary; else only the bucket that can hold key
     // 0xFFFFFFFF (the last one, if every key bit outside the buckets is one).
-    const bool single = (vary & ((1u << r.shift) - 1u)) == 0;
-    const uint32_t d_first = single ? ((a | (r.bmask << r.shift)) == 0xFFFFFFFFu ? r.bmask : nb) : 0u;
+    const bool single = (r.vary & ((1u << r.shift) - 1u)) == 0;
+    const uint32_t d_first = single ? ((r.all_and | (r.bmask << r.shift)) == 0xFFFFFFFFu ? r.bmask : nb) : 0u;
     int big = 0;
     for (uint32_t d = d_first + threadIdx.x; d < nb; d += blockDim.x) {
         if (cx[d] - (d ? cx[d - 1] : 0u) > 128) big |= 1;
         if (cy[d] - (d ? cy[d - 1] : 0u) > 128) big |= 2;
     }
-    const int bigx = __syncthreads_or(big & 1), bigy = __syncthreads_or(big & 2);
+    const bool bigx = __syncthreads_or(big & 1), bigy = __syncthreads_or(big & 2);
     if ((!bigx || !bigy) && d_first < nb) {
         const uint32_t sides = (bigx ? 0u : 1u) | (bigy ? 0u : 2u);
         for (uint32_t t = d_first + threadIdx.x; t < 2 * nb; t += blockDim.x) {
@@ -308,6 +332,29 @@ __device__ __forceinline__ DualSort dual_chunk_sort(const uint64_t *X, uint32_t 
     if (bigx) bitonic_words(Xo, nx);
     if (bigy) bitonic_words(Yo, ny);
     r.bitonic = bigx || bigy;
+}
+
+// chunk_sort of two chunks at once with one bucket function: X[0..nx) -> Xo
+// and Y[0..ny) -> Yo (nx, ny <= 8192), in the same order rules, with about
+// half the barriers of two calls.  Yo may be X's
+// buffer; Xo, X and Y must be distinct.  cnt holds kDualCntWords words:
+// afterwards the result's ex[d] / ey[d] is the end of bucket d of Xo / Yo
+// (unless bitonic).  red holds kDualRedWords scratch words.  ypads = all-ones
+// pad words among Y's.
+//
+// A Y chunk of one key (a hot key's block under skew: every increment would hit
+// one shared counter) is not sorted at all: y_single reports it, and the caller
+// pairs its words with X's run of that key.
+//
+// The buckets are the (at most) 11 highest key bits that differ within the two
+// chunks.  When no lower key bit differs, every bucket holds one key value and
+// needs no further order (ties stay in arbitrary order, which merge_join does
+// not depend on), except for payload order among key 0xFFFFFFFF tuples.
+__device__ __forceinline__ DualSort dual_chunk_sort(const uint64_t *X, uint32_t nx, uint64_t *Xo, const uint64_t *Y,
+                                                    uint32_t ny, uint64_t *Yo, uint32_t *cnt, uint32_t *red,
+                                                    uint32_t ypads) {
+    DualSort r = dual_analyze(X, nx, Y, ny, cnt, red, ypads);
+    dual_sort_rest(r, X, nx, Xo, Y, ny, Yo, cnt, red);
     return r;
 }
 
