@@ -492,6 +492,14 @@ static void window_progress(const std::vector<unsigned long long> &st, uint64_t 
     o->lat_p99 = pct(0.99);
 }
 
+// Smallest i >= 1 with T[i].ts_ms < T[i - 1].ts_ms, by atomicMin into *bad
+// (left as it is when the stream is ordered).  T: stream tuples as words
+// {ts, tuple}.
+static __global__ void ts_order_check(const uint64_t *__restrict__ T, uint64_t n, unsigned long long *bad) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x + 1; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        if (T[2 * i] < T[2 * (i - 1)]) atomicMin(bad, (unsigned long long)i);
+}
+
 int stream_join(Context *ctx, Family fam, int model, const adb_stream_tuple *R, uint64_t nR,
                 const adb_stream_tuple *S, uint64_t nS, const adb_join_params *p, adb_window_result *out,
                 adb_window_progress *progress, uint64_t max_windows, uint64_t *n_windows) {
@@ -511,11 +519,20 @@ int stream_join(Context *ctx, Family fam, int model, const adb_stream_tuple *R, 
     const uint64_t nwin = (tend - wbase) / W + 1;
     std::vector<uint64_t> rb(nwin + 1), sb(nwin + 1);
     {
+        // first tuple of each window: one binary search per boundary (log n
+        // timestamp reads instead of a pass over the streams)
+        auto first_at = [](const adb_stream_tuple *T, uint64_t lo, uint64_t hi, uint64_t lim) {
+            while (lo < hi) {
+                const uint64_t mid = lo + (hi - lo) / 2;
+                if (T[mid].ts_ms < lim) lo = mid + 1; else hi = mid;
+            }
+            return lo;
+        };
         uint64_t i = 0, k = 0;
-        for (uint64_t w = 0; w <= nwin; w++) {
+        for (uint64_t w = 0; w < nwin; w++) {
             const uint64_t lim = wbase + w * W;
-            while (i < nR && R[i].ts_ms < lim) i++;
-            while (k < nS && S[k].ts_ms < lim) k++;
+            i = first_at(R, i, nR, lim);
+            k = first_at(S, k, nS, lim);
             rb[w] = i;
             sb[w] = k;
         }
@@ -543,19 +560,40 @@ int stream_join(Context *ctx, Family fam, int model, const adb_stream_tuple *R, 
             uint64_t a, b;
             max_steps = std::max(max_steps, step_sizes(w, &a, &b));
         }
-    const size_t in_bytes = Workspace::need(nR + 1, 16) + Workspace::need(nS + 1, 16) +
+    const size_t in_bytes = Workspace::need(nR + 1, 16) + Workspace::need(nS + 1, 16) + Workspace::need(2, 8) +
                             (progress ? Workspace::need(3 * max_steps, 8) : 0);
     ADB_TRY(ctx->ws.reserve(in_bytes + eager_plan_bytes(plan) + 4096));
     uint64_t *dR = reinterpret_cast<uint64_t *>(ctx->ws.take<adb_stream_tuple>(nR + 1));
     uint64_t *dS = reinterpret_cast<uint64_t *>(ctx->ws.take<adb_stream_tuple>(nS + 1));
     unsigned long long *acc = ctx->ws.take<unsigned long long>(4);
+    unsigned long long *bad = ctx->ws.take<unsigned long long>(2);   // first out-of-order index of R, S
     unsigned long long *stamps = progress ? ctx->ws.take<unsigned long long>(3 * max_steps) : nullptr;
     std::vector<unsigned long long> h_stamps(progress ? 3 * max_steps : 0);
     EagerWindow win;
     take_window(ctx, plan, win);
-    if (nR) ADB_CK(cudaMemcpyAsync(dR, R, nR * 16, cudaMemcpyHostToDevice, st));
-    if (nS) ADB_CK(cudaMemcpyAsync(dS, S, nS * 16, cudaMemcpyHostToDevice, st));
+    ADB_TRY(h2d_copy(ctx, dR, R, nR * 16, st));
+    ADB_TRY(h2d_copy(ctx, dS, S, nS * 16, st));
+    // order of streams too long for the host check, on their device copies
+    const bool check_r = nR > kHostOrderCheck, check_s = nS > kHostOrderCheck;
+    if (check_r || check_s) {
+        ctx->h_res[0] = nR;
+        ctx->h_res[1] = nS;
+        ADB_CK(cudaMemcpyAsync(bad, ctx->h_res, 16, cudaMemcpyHostToDevice, st));
+        if (check_r) ts_order_check<<<ctx->num_sms * 4, 256, 0, st>>>(dR, nR, bad);
+        if (check_s) ts_order_check<<<ctx->num_sms * 4, 256, 0, st>>>(dS, nS, bad + 1);
+        ADB_CK(cudaGetLastError());
+        ctx->kernels += (check_r ? 1 : 0) + (check_s ? 1 : 0);
+        ADB_CK(cudaMemcpyAsync(ctx->h_res, bad, 16, cudaMemcpyDeviceToHost, st));
+    }
     ADB_CK(cudaStreamSynchronize(st));
+    if (check_r && ctx->h_res[0] < nR) {
+        set_error("R is not ordered by timestamp (index %llu)", (unsigned long long)ctx->h_res[0]);
+        return ADB_ERR_ARG;
+    }
+    if (check_s && ctx->h_res[1] < nS) {
+        set_error("S is not ordered by timestamp (index %llu)", (unsigned long long)ctx->h_res[1]);
+        return ADB_ERR_ARG;
+    }
 
     const auto wall0 = std::chrono::steady_clock::now();
     for (uint64_t w = 0; w < nwin; w++) {

@@ -69,6 +69,63 @@ int pinned_reserve(char **buf, size_t *cap, size_t bytes) {
     return ADB_OK;
 }
 
+int h2d_copy(Context *ctx, void *dst, const void *src, size_t bytes, cudaStream_t st) {
+    if (!bytes) return ADB_OK;
+    cudaPointerAttributes at{};
+    const bool pinned = cudaPointerGetAttributes(&at, src) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    constexpr int T = Context::kCopyWorkers;
+    constexpr size_t K = Context::kCopyChunk;
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int workers = (int)std::min<unsigned>(T, hw > 1 ? hw / 2 : 1u);
+    if (pinned || bytes < (16u << 20) || workers < 2) {
+        ADB_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+        return ADB_OK;
+    }
+    if (!ctx->h_copy) {
+        for (int t = 0; t < T; t++) {
+            ADB_CK(cudaStreamCreateWithFlags(&ctx->copy_st[t], cudaStreamNonBlocking));
+            for (auto &e : ctx->copy_ev[t]) ADB_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        }
+        ADB_CK(cudaEventCreateWithFlags(&ctx->copy_start, cudaEventDisableTiming));
+        if (cudaMallocHost(reinterpret_cast<void **>(&ctx->h_copy), (size_t)T * 2 * K) != cudaSuccess) {
+            cudaGetLastError();
+            ctx->h_copy = nullptr;
+            set_error("pinned staging buffer of %zu bytes", (size_t)T * 2 * K);
+            return ADB_ERR_OOM;
+        }
+    }
+    // the copies start after the work already queued on st (dst may be in use there)
+    ADB_CK(cudaEventRecord(ctx->copy_start, st));
+    for (int t = 0; t < workers; t++) ADB_CK(cudaStreamWaitEvent(ctx->copy_st[t], ctx->copy_start, 0));
+    const size_t chunks = (bytes + K - 1) / K;
+    std::vector<cudaError_t> errs(workers, cudaSuccess);
+    auto work = [&](int t) {
+        cudaError_t e = cudaSetDevice(ctx->device);
+        int k = 0;
+        for (size_t c = t; c < chunks && e == cudaSuccess; c += workers, k ^= 1) {
+            unsigned char *slot = ctx->h_copy + ((size_t)t * 2 + k) * K;
+            e = cudaEventSynchronize(ctx->copy_ev[t][k]);   // the slot's previous copy is done
+            if (e != cudaSuccess) break;
+            const size_t off = c * K, len = std::min(K, bytes - off);
+            memcpy(slot, static_cast<const unsigned char *>(src) + off, len);
+            e = cudaMemcpyAsync(static_cast<unsigned char *>(dst) + off, slot, len, cudaMemcpyHostToDevice,
+                                ctx->copy_st[t]);
+            if (e == cudaSuccess) e = cudaEventRecord(ctx->copy_ev[t][k], ctx->copy_st[t]);
+        }
+        errs[t] = e;
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < workers; t++) pool.emplace_back(work, t);
+    work(0);
+    for (auto &th : pool) th.join();
+    for (int t = 0; t < workers; t++) {
+        ADB_CK(errs[t]);
+        for (auto &e : ctx->copy_ev[t]) ADB_CK(cudaStreamWaitEvent(st, e, 0));   // work after this waits
+    }
+    return ADB_OK;
+}
+
 void Workspace::release() {
     if (base) cudaFree(base);
     base = nullptr;
@@ -131,6 +188,14 @@ void ctx_destroy(Context *c) {
     if (c->h_res) cudaFreeHost(c->h_res);
     if (c->h_stage) cudaFreeHost(c->h_stage);
     if (c->h_out) cudaFreeHost(c->h_out);
+    for (int t = 0; t < Context::kCopyWorkers; t++) {
+        if (c->copy_st[t]) cudaStreamSynchronize(c->copy_st[t]);
+        if (c->copy_st[t]) cudaStreamDestroy(c->copy_st[t]);
+        for (auto &e : c->copy_ev[t])
+            if (e) cudaEventDestroy(e);
+    }
+    if (c->copy_start) cudaEventDestroy(c->copy_start);
+    if (c->h_copy) cudaFreeHost(c->h_copy);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -419,8 +484,9 @@ int adb_join(const char *algo, const adb_tuple *R, uint64_t nR, const adb_tuple 
     uint64_t *dS = ctx->ws.take<uint64_t>(nS + 2);
     cudaStream_t st = ctx->stream;
     ADB_CK(cudaEventRecord(ctx->ev[4], st));
-    if (nR) ADB_CK(cudaMemcpyAsync(dR, R, nR * 8, cudaMemcpyHostToDevice, st));
-    if (nS) ADB_CK(cudaMemcpyAsync(dS, S, nS * 8, cudaMemcpyHostToDevice, st));
+    s = h2d_copy(ctx, dR, R, nR * 8, st);
+    if (s == ADB_OK) s = h2d_copy(ctx, dS, S, nS * 8, st);
+    if (s) return out->status = s;
     ADB_CK(cudaEventRecord(ctx->ev[5], st));
     DevJoin j{dR, nR, dS, nS};
     j.test_flags = p ? p->test_flags : 0;
@@ -448,10 +514,13 @@ int adb_stream_join_progress(const char *algo, const adb_stream_tuple *R, uint64
         return ADB_ERR_ARG;
     }
     if ((nR && !R) || (nS && !S) || (max_windows && !windows)) { set_error("NULL pointer"); return ADB_ERR_ARG; }
-    for (uint64_t i = 1; i < nR; i++)
-        if (R[i].ts_ms < R[i - 1].ts_ms) { set_error("R is not ordered by timestamp (index %llu)", (unsigned long long)i); return ADB_ERR_ARG; }
-    for (uint64_t i = 1; i < nS; i++)
-        if (S[i].ts_ms < S[i - 1].ts_ms) { set_error("S is not ordered by timestamp (index %llu)", (unsigned long long)i); return ADB_ERR_ARG; }
+    // order of short streams checked here (longer ones on the device, after their copy)
+    if (nR <= kHostOrderCheck)
+        for (uint64_t i = 1; i < nR; i++)
+            if (R[i].ts_ms < R[i - 1].ts_ms) { set_error("R is not ordered by timestamp (index %llu)", (unsigned long long)i); return ADB_ERR_ARG; }
+    if (nS <= kHostOrderCheck)
+        for (uint64_t i = 1; i < nS; i++)
+            if (S[i].ts_ms < S[i - 1].ts_ms) { set_error("S is not ordered by timestamp (index %llu)", (unsigned long long)i); return ADB_ERR_ARG; }
     int s;
     CtxLock held_ = ctx_acquire(&s);
     Context *ctx = held_.ctx;

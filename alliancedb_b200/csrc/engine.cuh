@@ -12,9 +12,17 @@
 
 namespace adb {
 
+struct Context;
+
 void set_error(const char *fmt, ...);
 // Grows the pinned host buffer *buf to at least `bytes` (its old contents are lost).
 int pinned_reserve(char **buf, size_t *cap, size_t bytes);
+// Host -> device copy of `bytes` from src to dst (device), ordered after the
+// work queued on st before it and before the work queued after it.  Pinned
+// sources and copies under 16 MiB are one cudaMemcpyAsync; larger pageable
+// sources go through pinned slots filled by host worker threads, so that the
+// host-side copy runs on several cores and overlaps the DMA.
+int h2d_copy(Context *ctx, void *dst, const void *src, size_t bytes, cudaStream_t st);
 
 #define ADB_CK(call)                                                                      \
     do {                                                                                  \
@@ -52,6 +60,10 @@ struct Workspace {
     void release();
 };
 
+// Stream tuples per side whose timestamp order adb_stream_join checks on the
+// host; longer streams are checked on the device after their copy.
+constexpr uint64_t kHostOrderCheck = 1ull << 16;
+
 struct Context {
     int device = -1;
     int num_sms = kNumSMs;
@@ -66,6 +78,14 @@ struct Context {
     size_t h_stage_cap = 0;
     char *h_out = nullptr;
     size_t h_out_cap = 0;
+    // staged host -> device copies of pageable memory (h2d_copy): per worker a
+    // stream, two pinned slots and an event per slot; made on first use
+    static constexpr int kCopyWorkers = 8;
+    static constexpr size_t kCopyChunk = 4u << 20;
+    cudaStream_t copy_st[kCopyWorkers] = {};
+    cudaEvent_t copy_ev[kCopyWorkers][2] = {};
+    cudaEvent_t copy_start = nullptr;
+    unsigned char *h_copy = nullptr;       // kCopyWorkers x 2 x kCopyChunk
     bool attrs_set = false;
     int kernels = 0;                       // kernels launched by the current call
     std::recursive_mutex mu;               // held by the call that uses this context

@@ -116,7 +116,10 @@ const char *adb_algo_name(int i, int *provided);
 
 /* Join two host-resident relations: copies R and S to the device (inside the
  * call), joins, and reads back the result.  Replaces the algos[] entry
- * `name`.  R and S are not modified. */
+ * `name`.  R and S are not modified.  Pinned (page-locked) relations are
+ * copied by DMA directly; pageable ones of 16 MiB or more go through pinned
+ * staging slots that host worker threads fill while earlier slots are in
+ * flight (the same for adb_stream_join's streams). */
 int adb_join(const char *algo, const adb_tuple *R, uint64_t nR, const adb_tuple *S, uint64_t nS,
              const adb_join_params *p, adb_join_result *out);
 
@@ -156,7 +159,10 @@ typedef struct adb_window_result {
  * ms.  Tuples are fed to the device in arrival micro-batches of
  * p->batch_tuples (default: one millisecond of stream) and each batch is
  * joined on arrival against the window's device-resident state (eager
- * join).  Writes up to max_windows results; *n_windows = windows seen. */
+ * join).  Writes up to max_windows results; *n_windows = windows seen.
+ * Streams that are not ordered by ts_ms are refused with ADB_ERR_ARG: up to
+ * 2^16 tuples per side before the device is touched, longer ones on the
+ * device right after their copy, before any window runs. */
 int adb_stream_join(const char *algo, const adb_stream_tuple *R, uint64_t nR,
                     const adb_stream_tuple *S, uint64_t nS, const adb_join_params *p,
                     adb_window_result *windows, uint64_t max_windows, uint64_t *n_windows);

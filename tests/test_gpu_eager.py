@@ -151,3 +151,39 @@ def test_stream_progress(oracle, algo, realtime):
         if realtime:
             assert t[-1] < 250 + 50      # the last batch is released near the window's end
             assert g.lat_p99 < 50        # a batch's results follow its release closely
+
+
+def test_long_streams_staged_copy_and_order_check(oracle):
+    """Streams above the direct-copy threshold (16 MiB per side) reach the
+    device through the staged host copy from pageable memory: the windows
+    equal those of the same streams in pinned memory (one direct copy) and the
+    oracle's join of each window.  A long stream out of timestamp order is
+    refused after its copy, with the first offending index."""
+    import torch
+    R, S = make_streams(1_300_000, 650.0, 1 << 18, 4, 14)   # ~2 s, 20.8 MB per side
+    assert R.nbytes > (16 << 20) and S.nbytes > (16 << 20)
+    p = adb.default_params(window_size=1000, batch_tuples=1600, nthreads=8)
+    got = adb.stream_join("SHJ_JM_NP", R, S, p)
+    Rp = torch.empty(R.nbytes, dtype=torch.uint8, pin_memory=True).numpy().view(adb.STREAM_TUPLE)
+    Sp = torch.empty(S.nbytes, dtype=torch.uint8, pin_memory=True).numpy().view(adb.STREAM_TUPLE)
+    Rp[:] = R
+    Sp[:] = S
+    pinned = adb.stream_join("SHJ_JM_NP", Rp, Sp, p)
+    assert [(w.n_r, w.n_s, w.count, w.checksum) for w in got] == \
+           [(w.n_r, w.n_s, w.count, w.checksum) for w in pinned]
+    w = got[0]
+    r = R[R["ts_ms"] < w.window_start_ms + 1000]
+    s = S[S["ts_ms"] < w.window_start_ms + 1000]
+    assert (w.count, w.checksum) == oracle.truth(adb.tuples(r["key"], r["payload"]),
+                                                 adb.tuples(s["key"], s["payload"]))
+    for side in ("R", "S"):
+        bad_r, bad_s = R.copy(), S.copy()
+        bad = bad_r if side == "R" else bad_s
+        bad["ts_ms"][700_001] = 0
+        with pytest.raises(adb.AdbError) as e:
+            adb.stream_join("SHJ_JM_NP", bad_r, bad_s, p)
+        assert e.value.status == adb.ADB_ERR_ARG
+        assert f"{side} is not ordered by timestamp (index 700001)" in str(e.value)
+    # the context is still usable
+    again = adb.stream_join("SHJ_JM_NP", R, S, p)
+    assert [(w.count, w.checksum) for w in again] == [(w.count, w.checksum) for w in got]

@@ -208,3 +208,20 @@ def test_single_key_block_with_all_ones_tuples(oracle, algo):
     sp[[10, 2000]] = 0xFFFFFFFF
     S = adb.tuples(sk, sp)
     check(oracle, algo, R, S)
+
+
+@pytest.mark.parametrize("algo", ["PRO", "NPO", "m-way"])
+def test_host_inputs_through_the_staged_copy(oracle, algo):
+    """Host relations above the direct-copy threshold (16 MiB) in pageable
+    memory reach the device through the staged copy: a ragged last 4 MiB
+    chunk, and a source that starts one tuple into its array (8-byte aligned
+    only), both equal the direct-address truth."""
+    n = (1 << 22) + 12345
+    R = adb.gen_pk(n, 31)
+    S = adb.gen_fk(n + 7, R, 0.0, 32)
+    assert S.nbytes > (16 << 20)
+    got = adb.join(algo, R, S)
+    assert (got.count, got.checksum) == oracle.pk_truth(R, S)
+    Sv = S[1:]
+    got = adb.join(algo, R, Sv)
+    assert (got.count, got.checksum) == oracle.pk_truth(R, Sv)
