@@ -63,22 +63,44 @@ enum { M_JM_NP = 0, M_JM_P = 1, M_JB_NP = 2, M_JB_P = 3, M_JBCR_NP = 4, M_JBCR_P
 // ---------------------------------------------------------------------------
 constexpr uint32_t kNoBatch = 0xFFFFFFFFu;   // batch field of an empty record
 
+// Sub-tables: 2^log2parts key groups (the JB / JBCR key split) x 2^log2members
+// members per group (JBCR: the group's threads).  JBCR replicates R to every
+// member of its key's group and sends each S tuple to one member chosen at
+// random (ContRandShuffler::push, hashing/helper/shuffler.cpp:143-168), so an
+// R tuple is inserted into, and probes, every member's sub-table, an S tuple
+// only its own member's; each pair still meets exactly once.
 struct ShjTables {
     ulonglong2 *tab[2];        // R, S: records {x = tuple word, y = arrival batch (low 32 bits)}
     uint32_t log2sub[2];       // slots per sub-table (log2)
-    uint32_t log2parts;        // sub-tables per side (log2)
+    uint32_t log2parts;        // key groups (log2)
+    uint32_t log2members;      // members per group (log2; 0 unless JBCR)
+    uint64_t seed;             // JBCR: the random member of each S tuple
 };
 
 __device__ __forceinline__ uint32_t shj_part(uint32_t key, uint32_t log2parts) {
     return log2parts ? (uint32_t)((key * 0x85EBCA6Bu) >> (32 - log2parts)) : 0u;
 }
 
-// Inserts tuple word w of arrival batch `batch` into side `side`'s table.
-__device__ __forceinline__ void shj_insert(const ShjTables &t, int side, uint64_t w, uint32_t batch, int *err) {
+// JBCR: the member of S tuple number sidx of the window (its arrival
+// position), a counter-based draw (SplitMix64 of seed and sidx), so insert and
+// probe agree without storing it.
+__device__ __forceinline__ uint32_t shj_member(const ShjTables &t, uint64_t sidx) {
+    if (!t.log2members) return 0u;
+    return (uint32_t)(fmix64(t.seed + 0x9E3779B97F4A7C15ULL * (sidx + 1)) >> (64 - t.log2members));
+}
+
+__device__ __forceinline__ uint64_t shj_sub(const ShjTables &t, int side, uint32_t key, uint32_t member) {
+    return ((((uint64_t)shj_part(key, t.log2parts) << t.log2members) | member) << t.log2sub[side]);
+}
+
+// Inserts tuple word w of arrival batch `batch` into member `member`'s
+// sub-table of side `side`.
+__device__ __forceinline__ void shj_insert(const ShjTables &t, int side, uint64_t w, uint32_t batch, uint32_t member,
+                                           int *err) {
     const uint32_t lo = t.log2sub[side];
     const uint64_t m = (1ULL << lo) - 1;
     const uint32_t key = tkey(w);
-    ulonglong2 *tab = t.tab[side] + ((uint64_t)shj_part(key, t.log2parts) << lo);
+    ulonglong2 *tab = t.tab[side] + shj_sub(t, side, key, member);
     uint64_t slot = npo_hash(key, lo);
     for (uint64_t tries = 0;; tries++) {
         unsigned int *bf = reinterpret_cast<unsigned int *>(&tab[slot].y);
@@ -91,14 +113,15 @@ __device__ __forceinline__ void shj_insert(const ShjTables &t, int side, uint64_
     }
 }
 
-// Probes side `side`'s table with tuple word w (of the other side) and adds the
-// matches whose arrival batch is <= max_batch.  r_probe: w is an R tuple.
+// Probes member `member`'s sub-table of side `side` with tuple word w (of the
+// other side) and adds the matches whose arrival batch is <= max_batch.
+// r_probe: w is an R tuple.
 __device__ __forceinline__ void shj_probe(const ShjTables &t, int side, uint64_t w, uint32_t max_batch, bool r_probe,
-                                          Acc &a) {
+                                          uint32_t member, Acc &a) {
     const uint32_t lo = t.log2sub[side];
     const uint64_t m = (1ULL << lo) - 1;
     const uint32_t key = tkey(w);
-    const ulonglong2 *tab = t.tab[side] + ((uint64_t)shj_part(key, t.log2parts) << lo);
+    const ulonglong2 *tab = t.tab[side] + shj_sub(t, side, key, member);
     uint64_t slot = npo_hash(key, lo);
     for (uint64_t tries = 0; tries <= m; tries++) {
         const ulonglong2 rec = tab[slot];
@@ -115,15 +138,22 @@ __device__ __forceinline__ void shj_probe(const ShjTables &t, int side, uint64_t
 // One micro-batch of one side (per-batch form): insert into the own table,
 // probe the other (which holds only earlier arrivals).  `in` holds elements of
 // `stride` 64-bit words with the tuple in the last word (1: plain tuples, 2:
-// adb_stream_tuple).
+// adb_stream_tuple); in[0] is tuple number `base` of its side in the window.
 __global__ void shj_batch(const uint64_t *__restrict__ in, uint32_t stride, uint64_t n, int side, uint32_t batch,
-                          ShjTables t, unsigned long long *acc, int *err) {
+                          uint64_t base, ShjTables t, unsigned long long *acc, int *err) {
     __shared__ uint64_t red[64];
     Acc a;
+    const uint32_t members = 1u << t.log2members;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t w = in[i * stride + (stride - 1)];
-        shj_insert(t, side, w, batch, err);                         // (1)/(3)
-        shj_probe(t, 1 - side, w, kNoBatch - 1, side == 0, a);     // (2)/(4)
+        if (side == 0) {   // R: every member of the group
+            for (uint32_t m = 0; m < members; m++) shj_insert(t, 0, w, batch, m, err);       // (1)
+            for (uint32_t m = 0; m < members; m++) shj_probe(t, 1, w, kNoBatch - 1, true, m, a);   // (2)
+        } else {           // S: its own member
+            const uint32_t m = shj_member(t, base + i);
+            shj_insert(t, 1, w, batch, m, err);                     // (3)
+            shj_probe(t, 0, w, kNoBatch - 1, false, m, a);          // (4)
+        }
     }
     block_flush(a, acc, red);
 }
@@ -137,7 +167,11 @@ __global__ void shj_insert_window(const uint64_t *__restrict__ R, uint64_t nR, c
         const bool isr = i < nR;
         const uint64_t k = isr ? i : i - nR;
         const uint64_t w = (isr ? R : S)[k * stride + (stride - 1)];
-        shj_insert(t, isr ? 0 : 1, w, (uint32_t)(k / (isr ? sr : ss)), err);
+        const uint32_t b = (uint32_t)(k / (isr ? sr : ss));
+        if (isr)
+            for (uint32_t m = 0; m < (1u << t.log2members); m++) shj_insert(t, 0, w, b, m, err);
+        else
+            shj_insert(t, 1, w, b, shj_member(t, k), err);
     }
 }
 
@@ -156,22 +190,37 @@ __global__ void shj_probe_window(const uint64_t *__restrict__ R, uint64_t nR, co
         const uint64_t w = (isr ? R : S)[k * stride + (stride - 1)];
         const uint32_t b = (uint32_t)(k / (isr ? sr : ss));
         if (isr) {
-            if (b) shj_probe(t, 1, w, b - 1, true, a);
+            if (b)
+                for (uint32_t m = 0; m < (1u << t.log2members); m++) shj_probe(t, 1, w, b - 1, true, m, a);
         } else {
-            shj_probe(t, 0, w, b, false, a);
+            shj_probe(t, 0, w, b, false, shj_member(t, k), a);
         }
     }
     block_flush(a, acc, red);
 }
 
+static uint32_t floor_log2(int v) {
+    uint32_t l = 0;
+    while ((1 << (l + 1)) <= v) l++;
+    return l;
+}
+
+// Key groups: JB one per thread, JBCR nthreads / group_size (both rounded
+// down to a power of two); JM, HS and the single-thread forms one table.
 static uint32_t shj_log2parts(int model, int nthreads, int group_size) {
     int parts = 1;
     if (model == M_JB_NP || model == M_JB_P) parts = nthreads > 0 ? nthreads : 1;
     if (model == M_JBCR_NP || model == M_JBCR_P)
         parts = std::max(1, (nthreads > 0 ? nthreads : 1) / std::max(1, group_size > 0 ? group_size : 1));
-    uint32_t l = 0;
-    while ((1 << (l + 1)) <= parts) l++;   // round down to a power of two
-    return l;
+    return floor_log2(parts);
+}
+
+// Members per group: JBCR's group_size (at most nthreads, rounded down to a
+// power of two); 1 otherwise.
+static uint32_t shj_log2members(int model, int nthreads, int group_size) {
+    if (model != M_JBCR_NP && model != M_JBCR_P) return 0;
+    const int n = nthreads > 0 ? nthreads : 1;
+    return floor_log2(std::max(1, std::min(n, group_size > 0 ? group_size : 1)));
 }
 
 static uint32_t shj_log2sub(uint64_t n, uint32_t log2parts) {
@@ -236,7 +285,7 @@ struct EagerWindow {
 
 struct EagerPlan {
     Family fam;
-    uint32_t log2parts;
+    uint32_t log2parts, log2members;
     uint32_t log2sub[2];
     uint64_t capR, capS;   // most tuples of one window
     uint64_t run_cap;      // PMJ: most tuples of one run
@@ -251,28 +300,31 @@ static EagerPlan plan_eager(Family fam, int model, int nthreads, int group_size,
     p.run_cap = run_cap;
     if (fam == Family::Shj) {
         p.log2parts = shj_log2parts(model, nthreads, group_size);
-        p.log2sub[0] = shj_log2sub(capR, p.log2parts);
-        p.log2sub[1] = shj_log2sub(capS, p.log2parts);
+        p.log2members = shj_log2members(model, nthreads, group_size);
+        p.log2sub[0] = shj_log2sub(capR, p.log2parts);                   // a member holds its group's whole R
+        p.log2sub[1] = shj_log2sub(capS, p.log2parts + p.log2members);   // and its random share of S
     }
     return p;
 }
 
 static size_t eager_plan_bytes(const EagerPlan &p) {
     if (p.fam == Family::Shj)
-        return Workspace::need(1ULL << (p.log2sub[0] + p.log2parts), 16) +
-               Workspace::need(1ULL << (p.log2sub[1] + p.log2parts), 16);
+        return Workspace::need(1ULL << (p.log2sub[0] + p.log2parts + p.log2members), 16) +
+               Workspace::need(1ULL << (p.log2sub[1] + p.log2parts + p.log2members), 16);
     return 2 * Workspace::need(p.capR + 1, 8) + 2 * Workspace::need(p.capS + 1, 8) +
            2 * Workspace::need(p.run_cap + 1, 8);
 }
 
-static void take_window(Context *ctx, const EagerPlan &p, EagerWindow &w) {
+static void take_window(Context *ctx, const EagerPlan &p, EagerWindow &w, uint64_t seed) {
     if (p.fam == Family::Shj) {
         for (int s = 0; s < 2; s++) {
-            w.tab_slots[s] = 1ULL << (p.log2sub[s] + p.log2parts);
+            w.tab_slots[s] = 1ULL << (p.log2sub[s] + p.log2parts + p.log2members);
             w.t.tab[s] = ctx->ws.take<ulonglong2>(w.tab_slots[s]);
             w.t.log2sub[s] = p.log2sub[s];
         }
         w.t.log2parts = p.log2parts;
+        w.t.log2members = p.log2members;
+        w.t.seed = seed;
     } else {
         for (int s = 0; s < 2; s++) {
             const uint64_t cap = s ? p.capS : p.capR;
@@ -300,17 +352,18 @@ static int grid_for(Context *ctx, uint64_t n) {
     return (int)(b < 1 ? 1 : (b > cap ? cap : b));
 }
 
-// SHJ: micro-batch k of each side, R first (shj() alternates R then S).
+// SHJ: micro-batch k of each side, R first (shj() alternates R then S); S[0]
+// is S tuple number s_base of the window.
 static int shj_step(Context *ctx, EagerWindow &w, const uint64_t *R, uint64_t nr, const uint64_t *S, uint64_t ns,
-                    uint32_t stride, uint32_t k, unsigned long long *acc) {
+                    uint64_t s_base, uint32_t stride, uint32_t k, unsigned long long *acc) {
     cudaStream_t st = ctx->stream;
     int *err = reinterpret_cast<int *>(acc + 2);
     if (nr) {
-        shj_batch<<<grid_for(ctx, nr), 256, 0, st>>>(R, stride, nr, 0, k, w.t, acc, err);
+        shj_batch<<<grid_for(ctx, nr), 256, 0, st>>>(R, stride, nr, 0, k, 0, w.t, acc, err);
         ctx->kernels++;
     }
     if (ns) {
-        shj_batch<<<grid_for(ctx, ns), 256, 0, st>>>(S, stride, ns, 1, k, w.t, acc, err);
+        shj_batch<<<grid_for(ctx, ns), 256, 0, st>>>(S, stride, ns, 1, k, s_base, w.t, acc, err);
         ctx->kernels++;
     }
     ADB_CK(cudaGetLastError());
@@ -366,8 +419,9 @@ static int pmj_step(Context *ctx, EagerWindow &w, const uint64_t *R, uint64_t nr
 }
 
 static int eager_step(Context *ctx, const EagerPlan &p, EagerWindow &w, const uint64_t *R, uint64_t nr,
-                      const uint64_t *S, uint64_t ns, uint32_t stride, uint32_t k, unsigned long long *acc) {
-    return p.fam == Family::Shj ? shj_step(ctx, w, R, nr, S, ns, stride, k, acc)
+                      const uint64_t *S, uint64_t ns, uint64_t s_base, uint32_t stride, uint32_t k,
+                      unsigned long long *acc) {
+    return p.fam == Family::Shj ? shj_step(ctx, w, R, nr, S, ns, s_base, stride, k, acc)
                                 : pmj_step(ctx, w, R, nr, S, ns, stride, acc);
 }
 
@@ -413,13 +467,13 @@ size_t eager_scratch(uint64_t nR, uint64_t nS, Family fam, int model, int nthrea
 }
 
 int run_eager(Context *ctx, const DevJoin &j, Family fam, int model, uint64_t batch, int nthreads, int group_size,
-              int progressive_step, uint64_t /*seed*/, unsigned long long *acc) {
+              int progressive_step, uint64_t seed, unsigned long long *acc) {
     uint64_t sr, ss;
     eager_steps(fam, j.nR, j.nS, batch, progressive_step, &sr, &ss);
     const uint64_t runs = std::max((j.nR + sr - 1) / sr, (j.nS + ss - 1) / ss);
     const EagerPlan p = plan_eager(fam, model, nthreads, group_size, j.nR, j.nS, std::max(j.nR, j.nS));
     EagerWindow w;
-    take_window(ctx, p, w);
+    take_window(ctx, p, w, seed);
     ADB_TRY(reset_window(ctx, p, w));
     ADB_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
     ADB_CK(cudaEventRecord(ctx->ev[2], ctx->stream));
@@ -430,7 +484,7 @@ int run_eager(Context *ctx, const DevJoin &j, Family fam, int model, uint64_t ba
         // the last step takes the left-over of both sides (localjoiner.cpp:575-590)
         const uint64_t r0 = std::min(j.nR, k * sr), r1 = k + 1 == runs ? j.nR : std::min(j.nR, (k + 1) * sr);
         const uint64_t s0 = std::min(j.nS, k * ss), s1 = k + 1 == runs ? j.nS : std::min(j.nS, (k + 1) * ss);
-        ADB_TRY(eager_step(ctx, p, w, j.R + r0, r1 - r0, j.S + s0, s1 - s0, 1, (uint32_t)k, acc));
+        ADB_TRY(eager_step(ctx, p, w, j.R + r0, r1 - r0, j.S + s0, s1 - s0, s0, 1, (uint32_t)k, acc));
     }
     return ADB_OK;
 }
@@ -570,7 +624,7 @@ int stream_join(Context *ctx, Family fam, int model, const adb_stream_tuple *R, 
     unsigned long long *stamps = progress ? ctx->ws.take<unsigned long long>(3 * max_steps) : nullptr;
     std::vector<unsigned long long> h_stamps(progress ? 3 * max_steps : 0);
     EagerWindow win;
-    take_window(ctx, plan, win);
+    take_window(ctx, plan, win, p ? p->seed : 0);
     ADB_TRY(h2d_copy(ctx, dR, R, nR * 16, st));
     ADB_TRY(h2d_copy(ctx, dS, S, nS * 16, st));
     // order of streams too long for the host check, on their device copies
@@ -621,7 +675,8 @@ int stream_join(Context *ctx, Family fam, int model, const adb_stream_tuple *R, 
             }
             if (k + 1 == steps) ADB_CK(cudaEventRecord(ctx->ev[4], st));
             if (stamp) stamp_kernel<<<1, 1, 0, st>>>(nullptr, stamps + 3 * k);
-            ADB_TRY(eager_step(ctx, plan, win, dR + 2 * a0, a1 - a0, dS + 2 * c0, c1 - c0, 2, (uint32_t)k, acc));
+            ADB_TRY(eager_step(ctx, plan, win, dR + 2 * a0, a1 - a0, dS + 2 * c0, c1 - c0, c0 - s0, 2, (uint32_t)k,
+                               acc));
             if (stamp) {
                 stamp_kernel<<<1, 1, 0, st>>>(acc, stamps + 3 * k + 1);
                 ctx->kernels += 2;

@@ -187,3 +187,24 @@ def test_long_streams_staged_copy_and_order_check(oracle):
     # the context is still usable
     again = adb.stream_join("SHJ_JM_NP", R, S, p)
     assert [(w.count, w.checksum) for w in again] == [(w.count, w.checksum) for w in got]
+
+
+@pytest.mark.parametrize("nthreads,group_size", [(8, 1), (8, 2), (8, 4), (8, 8), (6, 3), (4, 16)])
+@pytest.mark.parametrize("seed", [0, 12345])
+def test_jbcr_groups_members_and_seeds(oracle, nthreads, group_size, seed):
+    """JBCR: R replicated to every member of its key group, each S tuple sent
+    to one seeded random member.  Any group layout and seed gives the oracle's
+    join, and the per-batch form (progress) the same windows as the
+    throughput form."""
+    R = dup_streams(20000, 3000, 4, 5)
+    S = dup_streams(30000, 3000, 4, 6)
+    p = adb.default_params(nthreads=nthreads, group_size=group_size, seed=seed)
+    for algo in ("SHJ_JBCR_NP", "SHJ_JBCR_P"):
+        got = adb.join(algo, R, S, p)
+        assert (got.count, got.checksum) == oracle.truth(R, S), algo
+    Rs, Ss = make_streams(8000, 8.0, 800, 4, 15)
+    q = adb.default_params(window_size=500, batch_tuples=64, nthreads=nthreads, group_size=group_size, seed=seed)
+    plain = adb.stream_join("SHJ_JBCR_NP", Rs, Ss, q)
+    wins, _ = adb.stream_join("SHJ_JBCR_NP", Rs, Ss, q, progress=True)
+    assert [(w.count, w.checksum) for w in wins] == [(w.count, w.checksum) for w in plain]
+    assert sum(w.n_r for w in wins) == len(Rs)
