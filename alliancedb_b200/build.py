@@ -80,7 +80,7 @@ def build_oracle(ref: Path | None = None) -> Path:
     given) the reference's own joins under oracle/_ref/."""
     _run(["make", "-s", "-C", str(ROOT / "oracle"), "liboracle.so"])
     if ref is not None:
-        _run(["make", "-s", "-j8", "-C", str(ROOT / "oracle"), "ref", "read", "ck", f"REF_ROOT={ref}"])
+        _run(["make", "-s", "-j8", "-C", str(ROOT / "oracle"), "ref", "read", "ck", "wait", f"REF_ROOT={ref}"])
     return ORACLE_LIB
 
 

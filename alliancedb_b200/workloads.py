@@ -75,6 +75,28 @@ def ref_windows(algo: str, windows, threads: int, binary: str = "adb_ref_bench")
     return json.loads([ln for ln in out.splitlines() if ln.startswith("{")][-1])
 
 
+def ref_arrivals(algo: str, R, S, threads: int):
+    """The reference's own eager `algo` built with WAIT kept
+    (oracle/_ref/adb_ref_hash_wait) on one window of two STREAM_TUPLE arrays
+    whose payloads are their row numbers: every tuple is released at its
+    timestamp (ms from the window's first), so the call lasts the window;
+    returns the harness's JSON (count, call ms, last arrival, latency after
+    it), or None when that build is absent."""
+    ref = ROOT / "oracle" / "_ref" / "adb_ref_hash_wait"
+    if not ref.exists() or not len(R) or not len(S):
+        return None
+    t0 = int(min(R["ts_ms"][0], S["ts_ms"][0]))
+    with tempfile.TemporaryDirectory(dir=os.environ.get("ADB_TMP")) as tmp:
+        t = Path(tmp)
+        adb.tuples(R["key"], np.arange(len(R), dtype=np.uint32)).view(np.uint64).tofile(t / "R.bin")
+        adb.tuples(S["key"], np.arange(len(S), dtype=np.uint32)).view(np.uint64).tofile(t / "S.bin")
+        (R["ts_ms"].astype(np.uint64) - np.uint64(t0)).tofile(t / "tR.bin")
+        (S["ts_ms"].astype(np.uint64) - np.uint64(t0)).tofile(t / "tS.bin")
+        out = subprocess.run([str(ref), algo, "arrivals", *(str(t / f) for f in ("R.bin", "S.bin", "tR.bin", "tS.bin")),
+                              str(threads)], capture_output=True, text=True, timeout=600, check=True).stdout
+    return json.loads([ln for ln in out.splitlines() if ln.startswith("{")][-1])
+
+
 def _logu(rng, lo, hi, n):
     return np.floor(2.0 ** rng.uniform(lo, hi, size=n)).astype(np.uint64)
 
@@ -278,6 +300,16 @@ def bench_stream(args, cpu: bool = True):
                                    "sample": f"the reference's eager joins (WAIT off: throughput) on the first "
                                              f"1000 ms window ({len(w0[0][0])} + {len(w0[0][1])} tuples), one call "
                                              f"each, {th} threads"}
+            # latency: the same window with WAIT kept, each tuple released at its
+            # timestamp; the latency is the call's end after the last arrival
+            lat = {}
+            for algo in ("SHJ_JM_NP", "PMJ_JM_NP"):
+                d = ref_arrivals(algo, r0, s0, th)
+                if d is not None:
+                    lat[algo] = {"window_ms": d["ms"], "last_arrival_ms": d["last_arrival_ms"],
+                                 "latency_ms": d["latency_ms"], "count": d["count"]}
+            if lat:
+                out["cpu_baseline"]["latency_wait_on"] = lat
     return out
 
 

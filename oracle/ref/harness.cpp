@@ -16,6 +16,15 @@
 //       last three are param_t fields of the eager joins; defaults 1, 2, 2)
 //   adb_ref_bench <algo> windows <R.bin> <S.bin> <off.bin> <threads>
 //       many independent R/S window pairs joined one after the other (below)
+//   adb_ref_hash[_wait] <algo> arrivals <R.bin> <S.bin> <tsR.bin> <tsS.bin> <threads>
+//       one call on two relations whose tuples arrive over time (tsX.bin: one
+//       u64 ms offset per tuple, from the start of the call; payloadID = row).
+//       Built with the reference's WAIT on (adb_ref_hash_wait) its fetchers
+//       release each tuple once its time has passed (hashing/helper/
+//       fetcher.cpp:127-131, 164-168) on the time-stamp counter of
+//       hashing/timer/rdtsc.h; the offsets are converted to that counter at
+//       the rate measured here.  Prints count, the call's ms, the last arrival
+//       and the latency (call ms - last arrival ms).
 //   adb_ref_bench dump <n> <theta> <R.bin> <S.bin>
 //       writes the relations that `gen` would join (to check the restated
 //       generator against the benchmark's)
@@ -179,6 +188,59 @@ static int run_windows(join_fn fn, const std::string &algo, char **argv) {
     return 0;
 }
 
+#ifdef ADB_REF_FULL
+#include <x86intrin.h>
+
+// `arrivals` mode (above): one timed call, arrival times on the TSC.
+static int run_arrivals(join_fn fn, const std::string &algo, char **argv) {
+    std::vector<tuple_t> R0, S0;
+    std::vector<uint64_t> msR, msS;
+    if (!read_rel(argv[3], R0) || !read_rel(argv[4], S0) || !read_rel(argv[5], msR) || !read_rel(argv[6], msS) ||
+        msR.size() != R0.size() || msS.size() != S0.size())
+        return 2;
+    for (size_t i = 0; i < R0.size(); i++)
+        if ((uint64_t)(uint32_t)R0[i].payloadID != i) return 2;
+    for (size_t i = 0; i < S0.size(); i++)
+        if ((uint64_t)(uint32_t)S0[i].payloadID != i) return 2;
+    nthreads = std::max(1, atoi(argv[7]));
+    // counter ticks per ms
+    const auto c0 = std::chrono::steady_clock::now();
+    const uint64_t k0 = __rdtsc();
+    std::this_thread::sleep_for(std::chrono::milliseconds(200));
+    const uint64_t k1 = __rdtsc();
+    const double per_ms = (double)(k1 - k0) /
+                          std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - c0).count();
+    std::vector<uint64_t> tsR(R0.size() + 1, 0), tsS(S0.size() + 1, 0);
+    uint64_t last = 0;
+    for (size_t i = 0; i < R0.size(); i++) { tsR[i] = (uint64_t)(msR[i] * per_ms); last = std::max(last, msR[i]); }
+    for (size_t i = 0; i < S0.size(); i++) { tsS[i] = (uint64_t)(msS[i] * per_ms); last = std::max(last, msS[i]); }
+    param_t p;
+    memset((void *)&p, 0, sizeof(p));
+    p.nthreads = nthreads;
+    p.duplicate_num = 1;
+    p.progressive_step = 1;
+    p.merge_step = 2;
+    p.group_size = 2;
+    tuple_t *rt = alloc_rel(R0.size()), *st = alloc_rel(S0.size());
+    memcpy(rt, R0.data(), R0.size() * sizeof(tuple_t));
+    memcpy(st, S0.data(), S0.size() * sizeof(tuple_t));
+    relation_t relR{rt, R0.size(), nullptr}, relS{st, S0.size(), nullptr};
+    relation_payload_t payR{tsR.data(), R0.size()}, payS{tsS.data(), S0.size()};
+    relR.payload = &payR;
+    relS.payload = &payS;
+    const auto t0 = std::chrono::steady_clock::now();
+    result_t *res = fn(&relR, &relS, p);
+    const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if (!res) return 1;
+    printf("{\"algo\": \"%s\", \"n_r\": %zu, \"n_s\": %zu, \"threads\": %d, \"count\": %lld, "
+           "\"ms\": %.3f, \"last_arrival_ms\": %llu, \"latency_ms\": %.3f, \"tsc_ticks_per_ms\": %.0f}\n",
+           algo.c_str(), R0.size(), S0.size(), nthreads, (long long)res->totalresults, ms,
+           (unsigned long long)last, ms - (double)last, per_ms);
+    free(res);
+    return 0;
+}
+#endif
+
 int main(int argc, char **argv) {
     if (argc < 3) {
         fprintf(stderr, "usage: %s <algo> gen <n> <threads> <reps> | <algo> files <R> <S> <threads>\n", argv[0]);
@@ -202,6 +264,9 @@ int main(int argc, char **argv) {
         return 2;
     }
     if (std::string(argv[2]) == "windows" && argc >= 7) return run_windows(fn, algo, argv);
+#ifdef ADB_REF_FULL
+    if (std::string(argv[2]) == "arrivals" && argc >= 8) return run_arrivals(fn, algo, argv);
+#endif
     std::vector<tuple_t> R0, S0;
     int reps = 1, warmup = 0;
     int progressive_step = 1, merge_step = 2, group_size = 2;
