@@ -263,14 +263,22 @@ partition_pass(PassArgs a) {
         }
     };
 
-    // L2 prefetch of a whole flat tile (one bulk prefetch; paged input is not
-    // prefetched: one bulk prefetch per 512-byte page costs the SM's bulk-copy
-    // unit more than the latency it hides)
+    // L2 prefetch of a tile: flat input one bulk prefetch of the whole tile;
+    // paged input one 128-byte line prefetch per thread, four per page (a bulk
+    // prefetch per 512-byte page costs the SM's bulk-copy unit more than the
+    // latency it hides)
     auto prefetch_tile = [&](uint64_t t0) {
         if (t0 >= e) return;
         if (!kPaged && vec && tid == 0) {
             const uint64_t n = min(kStep, e - t0) & ~1ull;   // 16-byte multiple
             if (n) prefetch_l2(in.in + t0, (uint32_t)(n * 8));
+        }
+        if (kPaged && tid < (int)(kStep * 4)) {
+            const uint64_t li = t0 + (uint64_t)(tid >> 2);
+            if (li < e) {
+                const uint64_t *line = in.pages + (uint64_t)upage[li - b] * kPageTuples + (tid & 3) * 16;
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(line));
+            }
         }
     };
 
