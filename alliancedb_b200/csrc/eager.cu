@@ -546,11 +546,13 @@ static void window_progress(const std::vector<unsigned long long> &st, uint64_t 
     o->lat_p99 = pct(0.99);
 }
 
-// Smallest i >= 1 with T[i].ts_ms < T[i - 1].ts_ms, by atomicMin into *bad
-// (left as it is when the stream is ordered).  T: stream tuples as words
-// {ts, tuple}.
-static __global__ void ts_order_check(const uint64_t *__restrict__ T, uint64_t n, unsigned long long *bad) {
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x + 1; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+// Smallest i in [max(lo, 1), hi) with T[i].ts_ms < T[i - 1].ts_ms, by
+// atomicMin into *bad (left as it is when that range is ordered).  T: stream
+// tuples as words {ts, tuple}.
+static __global__ void ts_order_check(const uint64_t *__restrict__ T, uint64_t lo, uint64_t hi,
+                                      unsigned long long *bad) {
+    for (uint64_t i = max(lo, (uint64_t)1) + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < hi;
+         i += (uint64_t)gridDim.x * blockDim.x)
         if (T[2 * i] < T[2 * (i - 1)]) atomicMin(bad, (unsigned long long)i);
 }
 
@@ -625,28 +627,62 @@ int stream_join(Context *ctx, Family fam, int model, const adb_stream_tuple *R, 
     std::vector<unsigned long long> h_stamps(progress ? 3 * max_steps : 0);
     EagerWindow win;
     take_window(ctx, plan, win, p ? p->seed : 0);
-    ADB_TRY(h2d_copy(ctx, dR, R, nR * 16, st));
-    ADB_TRY(h2d_copy(ctx, dS, S, nS * 16, st));
-    // order of streams too long for the host check, on their device copies
+    // Throughput form without progress, streams in pinned memory: window w + 1's
+    // tuples are copied (one DMA per side) while window w is joined.  Otherwise
+    // both streams are copied first (pageable ones through the staged copy,
+    // whose host threads work best on one large copy).  Streams too long for
+    // the host's order check are checked on their device copies, rows [lo, hi)
+    // at a time, into bad[] (read back as h_res[8], h_res[9]).
+    auto is_pinned = [](const void *ptr) {
+        cudaPointerAttributes at{};
+        const bool pinned = cudaPointerGetAttributes(&at, ptr) == cudaSuccess && at.type == cudaMemoryTypeHost;
+        cudaGetLastError();
+        return pinned;
+    };
+    const bool pipelined = !realtime && !progress && (!nR || is_pinned(R)) && (!nS || is_pinned(S));
     const bool check_r = nR > kHostOrderCheck, check_s = nS > kHostOrderCheck;
-    if (check_r || check_s) {
-        ctx->h_res[0] = nR;
-        ctx->h_res[1] = nS;
-        ADB_CK(cudaMemcpyAsync(bad, ctx->h_res, 16, cudaMemcpyHostToDevice, st));
-        if (check_r) ts_order_check<<<ctx->num_sms * 4, 256, 0, st>>>(dR, nR, bad);
-        if (check_s) ts_order_check<<<ctx->num_sms * 4, 256, 0, st>>>(dS, nS, bad + 1);
-        ADB_CK(cudaGetLastError());
-        ctx->kernels += (check_r ? 1 : 0) + (check_s ? 1 : 0);
-        ADB_CK(cudaMemcpyAsync(ctx->h_res, bad, 16, cudaMemcpyDeviceToHost, st));
-    }
-    ADB_CK(cudaStreamSynchronize(st));
-    if (check_r && ctx->h_res[0] < nR) {
-        set_error("R is not ordered by timestamp (index %llu)", (unsigned long long)ctx->h_res[0]);
-        return ADB_ERR_ARG;
-    }
-    if (check_s && ctx->h_res[1] < nS) {
-        set_error("S is not ordered by timestamp (index %llu)", (unsigned long long)ctx->h_res[1]);
-        return ADB_ERR_ARG;
+    auto order_check = [&](uint64_t r_lo, uint64_t r_hi, uint64_t s_lo, uint64_t s_hi) {
+        if (check_r && r_hi > r_lo) {
+            ts_order_check<<<ctx->num_sms * 4, 256, 0, st>>>(dR, r_lo, r_hi, bad);
+            ctx->kernels++;
+        }
+        if (check_s && s_hi > s_lo) {
+            ts_order_check<<<ctx->num_sms * 4, 256, 0, st>>>(dS, s_lo, s_hi, bad + 1);
+            ctx->kernels++;
+        }
+        return cudaGetLastError();
+    };
+    auto order_error = [&]() {
+        if (check_r && ctx->h_res[8] < nR) {
+            set_error("R is not ordered by timestamp (index %llu)", (unsigned long long)ctx->h_res[8]);
+            return true;
+        }
+        if (check_s && ctx->h_res[9] < nS) {
+            set_error("S is not ordered by timestamp (index %llu)", (unsigned long long)ctx->h_res[9]);
+            return true;
+        }
+        return false;
+    };
+    // window w's rows and the pair across its first boundary, copied without
+    // waiting for the windows before it (their rows are elsewhere)
+    auto copy_window = [&](uint64_t w) -> int {
+        ADB_TRY(h2d_copy(ctx, dR + 2 * rb[w], R + rb[w], (rb[w + 1] - rb[w]) * 16, st, false));
+        ADB_TRY(h2d_copy(ctx, dS + 2 * sb[w], S + sb[w], (sb[w + 1] - sb[w]) * 16, st, false));
+        ADB_CK(order_check(rb[w], rb[w + 1], sb[w], sb[w + 1]));
+        return ADB_OK;
+    };
+    ctx->h_res[8] = nR;
+    ctx->h_res[9] = nS;
+    ADB_CK(cudaMemcpyAsync(bad, ctx->h_res + 8, 16, cudaMemcpyHostToDevice, st));
+    if (pipelined) {
+        if (nwin) ADB_TRY(copy_window(0));
+    } else {
+        ADB_TRY(h2d_copy(ctx, dR, R, nR * 16, st));
+        ADB_TRY(h2d_copy(ctx, dS, S, nS * 16, st));
+        ADB_CK(order_check(0, nR, 0, nS));
+        ADB_CK(cudaMemcpyAsync(ctx->h_res + 8, bad, 16, cudaMemcpyDeviceToHost, st));
+        ADB_CK(cudaStreamSynchronize(st));
+        if (order_error()) return ADB_ERR_ARG;
     }
 
     const auto wall0 = std::chrono::steady_clock::now();
@@ -685,8 +721,11 @@ int stream_join(Context *ctx, Family fam, int model, const adb_stream_tuple *R, 
         if (stamp) ADB_CK(cudaMemcpyAsync(h_stamps.data(), stamps, 3 * steps * 8, cudaMemcpyDeviceToHost, st));
         const auto close = std::chrono::steady_clock::now();
         ADB_CK(cudaMemcpyAsync(ctx->h_res, acc, 32, cudaMemcpyDeviceToHost, st));
+        if (pipelined) ADB_CK(cudaMemcpyAsync(ctx->h_res + 8, bad, 16, cudaMemcpyDeviceToHost, st));
         ADB_CK(cudaEventRecord(ctx->ev[5], st));
-        ADB_CK(cudaStreamSynchronize(st));
+        if (pipelined && w + 1 < nwin) ADB_TRY(copy_window(w + 1));   // while window w runs
+        ADB_CK(cudaEventSynchronize(ctx->ev[5]));
+        if (pipelined && order_error()) return ADB_ERR_ARG;
         if (ctx->h_res[2]) {
             set_error("device table overflow in window %llu", (unsigned long long)w);
             return ADB_ERR_DEVICE;

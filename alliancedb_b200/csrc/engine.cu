@@ -69,7 +69,19 @@ int pinned_reserve(char **buf, size_t *cap, size_t bytes) {
     return ADB_OK;
 }
 
-int h2d_copy(Context *ctx, void *dst, const void *src, size_t bytes, cudaStream_t st) {
+static int copy_init(Context *ctx) {
+    if (ctx->copy_done) return ADB_OK;
+    constexpr int T = Context::kCopyWorkers;
+    for (int t = 0; t < T; t++) {
+        ADB_CK(cudaStreamCreateWithFlags(&ctx->copy_st[t], cudaStreamNonBlocking));
+        for (auto &e : ctx->copy_ev[t]) ADB_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    ADB_CK(cudaEventCreateWithFlags(&ctx->copy_start, cudaEventDisableTiming));
+    ADB_CK(cudaEventCreateWithFlags(&ctx->copy_done, cudaEventDisableTiming));
+    return ADB_OK;
+}
+
+int h2d_copy(Context *ctx, void *dst, const void *src, size_t bytes, cudaStream_t st, bool after_st) {
     if (!bytes) return ADB_OK;
     cudaPointerAttributes at{};
     const bool pinned = cudaPointerGetAttributes(&at, src) == cudaSuccess && at.type == cudaMemoryTypeHost;
@@ -79,25 +91,27 @@ int h2d_copy(Context *ctx, void *dst, const void *src, size_t bytes, cudaStream_
     const unsigned hw = std::thread::hardware_concurrency();
     const int workers = (int)std::min<unsigned>(T, hw > 1 ? hw / 2 : 1u);
     if (pinned || bytes < (16u << 20) || workers < 2) {
-        ADB_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+        if (after_st) {
+            ADB_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+            return ADB_OK;
+        }
+        ADB_TRY(copy_init(ctx));
+        ADB_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->copy_st[0]));
+        ADB_CK(cudaEventRecord(ctx->copy_done, ctx->copy_st[0]));
+        ADB_CK(cudaStreamWaitEvent(st, ctx->copy_done, 0));
         return ADB_OK;
     }
-    if (!ctx->h_copy) {
-        for (int t = 0; t < T; t++) {
-            ADB_CK(cudaStreamCreateWithFlags(&ctx->copy_st[t], cudaStreamNonBlocking));
-            for (auto &e : ctx->copy_ev[t]) ADB_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        }
-        ADB_CK(cudaEventCreateWithFlags(&ctx->copy_start, cudaEventDisableTiming));
-        if (cudaMallocHost(reinterpret_cast<void **>(&ctx->h_copy), (size_t)T * 2 * K) != cudaSuccess) {
-            cudaGetLastError();
-            ctx->h_copy = nullptr;
-            set_error("pinned staging buffer of %zu bytes", (size_t)T * 2 * K);
-            return ADB_ERR_OOM;
-        }
+    ADB_TRY(copy_init(ctx));
+    if (!ctx->h_copy && cudaMallocHost(reinterpret_cast<void **>(&ctx->h_copy), (size_t)T * 2 * K) != cudaSuccess) {
+        cudaGetLastError();
+        ctx->h_copy = nullptr;
+        set_error("pinned staging buffer of %zu bytes", (size_t)T * 2 * K);
+        return ADB_ERR_OOM;
     }
-    // the copies start after the work already queued on st (dst may be in use there)
-    ADB_CK(cudaEventRecord(ctx->copy_start, st));
-    for (int t = 0; t < workers; t++) ADB_CK(cudaStreamWaitEvent(ctx->copy_st[t], ctx->copy_start, 0));
+    if (after_st) {   // the copies start after the work already queued on st (dst may be in use there)
+        ADB_CK(cudaEventRecord(ctx->copy_start, st));
+        for (int t = 0; t < workers; t++) ADB_CK(cudaStreamWaitEvent(ctx->copy_st[t], ctx->copy_start, 0));
+    }
     const size_t chunks = (bytes + K - 1) / K;
     std::vector<cudaError_t> errs(workers, cudaSuccess);
     auto work = [&](int t) {
@@ -195,6 +209,7 @@ void ctx_destroy(Context *c) {
             if (e) cudaEventDestroy(e);
     }
     if (c->copy_start) cudaEventDestroy(c->copy_start);
+    if (c->copy_done) cudaEventDestroy(c->copy_done);
     if (c->h_copy) cudaFreeHost(c->h_copy);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;

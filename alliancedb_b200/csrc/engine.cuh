@@ -17,12 +17,14 @@ struct Context;
 void set_error(const char *fmt, ...);
 // Grows the pinned host buffer *buf to at least `bytes` (its old contents are lost).
 int pinned_reserve(char **buf, size_t *cap, size_t bytes);
-// Host -> device copy of `bytes` from src to dst (device), ordered after the
-// work queued on st before it and before the work queued after it.  Pinned
-// sources and copies under 16 MiB are one cudaMemcpyAsync; larger pageable
-// sources go through pinned slots filled by host worker threads, so that the
-// host-side copy runs on several cores and overlaps the DMA.
-int h2d_copy(Context *ctx, void *dst, const void *src, size_t bytes, cudaStream_t st);
+// Host -> device copy of `bytes` from src to dst (device), ordered before the
+// work queued on st after it and, with after_st, after the work queued on st
+// before it (without: dst is not in use there, and the copy overlaps that
+// work).  Pinned sources and copies under 16 MiB are one cudaMemcpyAsync;
+// larger pageable sources go through pinned slots filled by host worker
+// threads, so that the host-side copy runs on several cores and overlaps the
+// DMA.  src must stay unchanged until st has passed the copy.
+int h2d_copy(Context *ctx, void *dst, const void *src, size_t bytes, cudaStream_t st, bool after_st = true);
 
 #define ADB_CK(call)                                                                      \
     do {                                                                                  \
@@ -84,7 +86,7 @@ struct Context {
     static constexpr size_t kCopyChunk = 4u << 20;
     cudaStream_t copy_st[kCopyWorkers] = {};
     cudaEvent_t copy_ev[kCopyWorkers][2] = {};
-    cudaEvent_t copy_start = nullptr;
+    cudaEvent_t copy_start = nullptr, copy_done = nullptr;
     unsigned char *h_copy = nullptr;       // kCopyWorkers x 2 x kCopyChunk
     bool attrs_set = false;
     int kernels = 0;                       // kernels launched by the current call

@@ -161,8 +161,10 @@ typedef struct adb_window_result {
  * joined on arrival against the window's device-resident state (eager
  * join).  Writes up to max_windows results; *n_windows = windows seen.
  * Streams that are not ordered by ts_ms are refused with ADB_ERR_ARG: up to
- * 2^16 tuples per side before the device is touched, longer ones on the
- * device right after their copy, before any window runs. */
+ * 2^16 tuples per side before the device is touched, longer ones on their
+ * device copies (in the throughput form on pinned streams window by window,
+ * as each window's tuples arrive while the window before it is joined;
+ * results written before the refusal are then not valid). */
 int adb_stream_join(const char *algo, const adb_stream_tuple *R, uint64_t nR,
                     const adb_stream_tuple *S, uint64_t nS, const adb_join_params *p,
                     adb_window_result *windows, uint64_t max_windows, uint64_t *n_windows);
