@@ -86,7 +86,7 @@ smj_items(SmjArgs a) {
     uint64_t *bar = reinterpret_cast<uint64_t *>(ptab + 4 * kSmjTabEntries);
     uint64_t *red = bar + 2;                                 // 96 u64 (192 u32 of sort scratch)
     SmjRec *rec = reinterpret_cast<SmjRec *>(red + 96);      // [2]
-    __shared__ uint32_t runn;                                // length of R's run of a single S key
+    __shared__ uint32_t runn[2];   // length of R's run of a single S key, per item parity
 
     const uint32_t n_items = *a.n_items;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -166,7 +166,10 @@ smj_items(SmjArgs a) {
         __syncwarp();
     };
 
-    if (threadIdx.x == 0) mbar_init(bar, 1);
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        runn[0] = runn[1] = 0;
+    }
     if (warp == kCtl) {
         take(&rec[0]);
         table(&rec[0], ptab);
@@ -184,6 +187,7 @@ smj_items(SmjArgs a) {
         const uint32_t *tpk = tpg + kSmjTabEntries;
         const uint32_t nrpg = cr.nrpg, np = cr.nrpg + cr.nspg;
         const uint32_t rslots = cr.rslots, sslots = cr.sslots, rpad = cr.rpad, spad = cr.spad;
+        if (threadIdx.x == 0) runn[cur ^ 1] = 0;   // the next item's (this item's was zeroed the same way)
 
         // --- R chunk -> A and S block -> C, one bulk copy per page, page slots
         //     16-byte aligned (a page takes its count rounded up to even); the
@@ -211,12 +215,11 @@ smj_items(SmjArgs a) {
         // dropping as many words as there are pads is exact.  An S block of one
         // key K is not sorted, and neither is R: R's run of K is gathered into B.
         uint32_t *red32 = reinterpret_cast<uint32_t *>(red);
-        if (threadIdx.x == 0) runn = 0;   // read after the analysis barrier
         DualSort ds = dual_analyze(A, rslots, C, sslots, cnt, red32, spad);
         if (ds.y_single) {
             for (uint32_t i = threadIdx.x; i < rslots; i += blockDim.x) {
                 const uint64_t v = A[i];   // pads are all-ones words: K < 0xFFFFFFFF never meets them
-                if (tkey(v) == ds.y_key) B[atomicAdd(&runn, 1u)] = v;
+                if (tkey(v) == ds.y_key) B[atomicAdd(&runn[cur], 1u)] = v;
             }
             __syncthreads();
         } else {
@@ -247,8 +250,8 @@ smj_items(SmjArgs a) {
                                                           sslots - (ds.nb ? ds.ey[ds.nb - 1] : 0u) != spad);
         if (ds.y_single) {
             // the S block is one key K (a hot key under skew), left unsorted in C
-            // with its pads: every S word but the pads meets R's run of K, B[0..runn)
-            const uint32_t nrun = runn;
+            // with its pads: every S word but the pads meets R's run of K, B[0..runn[cur])
+            const uint32_t nrun = runn[cur];
             for (uint32_t j = threadIdx.x; j < sslots && warp != kCtl && nrun; j += kWork) {
                 const uint64_t s = C[j];
                 if (s == ~0ULL) continue;   // a pad
