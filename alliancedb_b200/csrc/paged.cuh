@@ -127,7 +127,7 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x, int lane) {
 // unit of a segment).  Per tile of up to kPTile tuples:
 //   A  every thread ranks its tuples within their digit (shared atomics on
 //      cnt[tile parity][d]);
-//   B  warp 0 (up to 128 digits, F / 32 per lane) or warps 0 .. F/32 - 1 (one
+//   B  warp 0 (up to 32 digits, one per lane) or warps 0 .. F/32 - 1 (one
 //      digit per lane) turn the counts into the tile's digit runs (toff), take
 //      the pages each digit's stream needs from the CTA's pool, and advance
 //      the streams (npos = next free slot of the digit's current page, kNone
@@ -140,7 +140,7 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x, int lane) {
 // Consecutive stage slots of a digit go to consecutive addresses, so warps
 // store contiguous runs; a run's partial first and last 32-byte sectors are
 // completed by the neighbouring tiles of the same stream while the line is
-// still in L2.  Three barriers per tile (four above 128 digits); the next
+// still in L2.  Three barriers per tile (four above 32 digits); the next
 // tile's loads are in flight during D.  kMode: 0 flat input, 1 paged input
 // (pass 2), 2 segmented flat input (batched windows).
 template <int kMode, int kThreads>
@@ -297,12 +297,13 @@ partition_pass(PassArgs a) {
             if (k & 1) rk[k / 2] |= r << 16; else rk[k / 2] = r;
         }
         __syncthreads();
-        // B. digit runs of the tile, pages, stream positions.  Up to 128 digits
-        //    warp 0 alone (lane l: digits l*q .. l*q + q - 1, q = F / 32), above
-        //    that warp w < F / 32 takes digits 32w .. 32w + 31, one per lane, and
-        //    the warps' totals are combined through shared memory (one extra
-        //    barrier).  New pages get their log entry in D, from the thread that
-        //    writes their first slot.
+        // B. digit runs of the tile, pages, stream positions.  Up to 32 digits
+        //    warp 0 alone, one per lane; above that warp w < F / 32 takes digits
+        //    32w .. 32w + 31, one per lane, and the warps' totals are combined
+        //    through shared memory (one extra barrier, which costs less than warp
+        //    0 walking 2 or 4 digits per lane while the CTA waits: at 2^27 both
+        //    passes of PRO gain, pass 2 1.232 -> 1.170 ms).  New pages get their
+        //    log entry in D, from the thread that writes their first slot.
         auto run_digit = [&](uint32_t d, uint32_t L, uint32_t p, uint32_t off, uint32_t first) {
             const uint32_t room = p == kNone ? 0u : kPageTuples - (p & (kPageTuples - 1));
             c[d] = 0;
@@ -327,8 +328,8 @@ partition_pass(PassArgs a) {
             const uint32_t room = p == kNone ? 0u : kPageTuples - (p & (kPageTuples - 1));
             return L > room ? (L - room + kPageTuples - 1) / kPageTuples : 0u;
         };
-        if (F <= 128) {
-            constexpr int kQ = 4;
+        if (F <= 32) {
+            constexpr int kQ = 1;   // digits per lane
             const uint32_t q = (F + 31) / 32;
             if (tid < 32) {
                 uint32_t Ls[kQ], Ps[kQ], sumL = 0, sumN = 0;
