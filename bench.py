@@ -400,7 +400,7 @@ def main():
     if args.workload != "join":
         from alliancedb_b200 import workloads
         line = {"batch": workloads.bench_batch, "serve": workloads.bench_serve,
-                "stream": workloads.bench_stream}[args.workload](args)
+                "stream": workloads.bench_stream}[args.workload](args, cpu=not args.no_cpu)
         print(json.dumps(line), flush=True)
         return
 
