@@ -57,13 +57,13 @@ ALG_BYTES = {"PRO": 24, "RJ_st": 24, "PRH": 24, "PRHO": 24, "NPO": 16, "NPO_st":
 # launch is that figure times the launch's tuples: the kernels stream every
 # tuple once, so traffic grows in proportion.
 KERNELS = {
-    "radix": {0: ("partition_pass<0,512> (pass 1)", 16, (270285568 + 214802176) / 2**25),
-              1: ("partition_pass<1,512> (pass 2)", 16, (273331456 + 214424576) / 2**25),
-              3: ("radix_join_items<Chain>", 8, (273641984 + 7539456) / 2**25)},
+    "radix": {0: ("partition_pass<0,512> (pass 1)", 16, (270269696 + 214559744) / 2**25),
+              1: ("partition_pass<1,512> (pass 2)", 16, (276501504 + 214193152) / 2**25),
+              3: ("radix_join_items<Chain>", 8, (273603584 + 3484416) / 2**25)},
     "npo": {0: ("npo_build", 8, None), 3: ("npo_probe", 8, None)},
     "smj": {0: ("partition_pass (both passes)", 32,
                 (271074048 + 215111680 + 279591680 + 219554048) / 2**25),
-            3: ("smj_items", 8, (281795584 + 3697664) / 2**25)},
+            3: ("smj_items", 8, (281787648 + 3820288) / 2**25)},
 }
 
 
