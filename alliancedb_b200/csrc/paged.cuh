@@ -425,10 +425,15 @@ partition_pass(PassArgs a) {
         // its B / C run after the next barrier, when every thread is past D
     }
     __syncthreads();
-    // E. fill of each digit's last page
+    // E. fill of each digit's last page; an odd fill gets the all-ones word in
+    //    its next slot, so that a 16-byte multiple copy of the page carries a
+    //    pad that sorts last (every other page of a stream is full)
     for (uint32_t d = tid; d < F; d += kThreads) {
         const uint32_t p = npos[d];
-        if (p != kNone && (p & (kPageTuples - 1))) o.pcount[p / kPageTuples] = (uint8_t)(p & (kPageTuples - 1));
+        if (p != kNone && (p & (kPageTuples - 1))) {
+            o.pcount[p / kPageTuples] = (uint8_t)(p & (kPageTuples - 1));
+            if (p & 1) o.pages[p] = ~0ULL;
+        }
     }
     // F. pages per digit of this CTA (its log was written by this block)
     const uint32_t used = misc[0];

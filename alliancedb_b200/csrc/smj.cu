@@ -191,8 +191,9 @@ smj_items(SmjArgs a) {
 
         // --- R chunk -> A and S block -> C, one bulk copy per page, page slots
         //     16-byte aligned (a page takes its count rounded up to even); the
-        //     pad slot behind an odd page is set to the all-ones word afterwards,
-        //     which sorts last and is cut off by count
+        //     pad slot behind an odd page arrives holding the all-ones word (the
+        //     partition pass wrote it there), which sorts last and is cut off
+        //     by count
         for (uint32_t k = threadIdx.x; k < np; k += blockDim.x) {
             const uint32_t v = tpk[k], c = v & 0xFFu;
             if (c) {
@@ -204,11 +205,6 @@ smj_items(SmjArgs a) {
         }
         if (!mbar_wait(bar, phase) || a.waits_run_out) atomicExch(a.err, 1);
         phase ^= 1;
-        __syncthreads();
-        for (uint32_t k = threadIdx.x; k < np; k += blockDim.x) {
-            const uint32_t v = tpk[k], c = v & 0xFFu;
-            if (c & 1) (k < nrpg ? A : C)[(v >> 8) + c] = ~0ULL;
-        }
         __syncthreads();
         // sorted R (+ pads) in B, sorted S (+ pads) in A; the pads are the last
         // words of each run and a real all-ones tuple is the same word, so
