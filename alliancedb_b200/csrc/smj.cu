@@ -203,9 +203,10 @@ smj_items(SmjArgs a) {
                          ((c + 1) & ~1u) * 8, bar);
             }
         }
+        // every thread waits on the mbarrier itself, which makes the copied
+        // words visible to it: no block barrier before the analysis
         if (!mbar_wait(bar, phase) || a.waits_run_out) atomicExch(a.err, 1);
         phase ^= 1;
-        __syncthreads();
         // sorted R (+ pads) in B, sorted S (+ pads) in A; the pads are the last
         // words of each run and a real all-ones tuple is the same word, so
         // dropping as many words as there are pads is exact.  An S block of one

@@ -311,12 +311,16 @@ __device__ __forceinline__ void dual_sort_rest(DualSort &r, const uint64_t *X, u
     // 0xFFFFFFFF (the last one, if every key bit outside the buckets is one).
     const bool single = (r.vary & ((1u << r.shift) - 1u)) == 0;
     const uint32_t d_first = single ? ((r.all_and | (r.bmask << r.shift)) == 0xFFFFFFFFu ? r.bmask : nb) : 0u;
-    int big = 0;
-    for (uint32_t d = d_first + threadIdx.x; d < nb; d += blockDim.x) {
-        if (cx[d] - (d ? cx[d - 1] : 0u) > 128) big |= 1;
-        if (cy[d] - (d ? cy[d - 1] : 0u) > 128) big |= 2;
+    bool bigx = false, bigy = false;
+    if (d_first < nb) {   // (block-uniform) some bucket may hold several keys
+        int big = 0;
+        for (uint32_t d = d_first + threadIdx.x; d < nb; d += blockDim.x) {
+            if (cx[d] - (d ? cx[d - 1] : 0u) > 128) big |= 1;
+            if (cy[d] - (d ? cy[d - 1] : 0u) > 128) big |= 2;
+        }
+        bigx = __syncthreads_or(big & 1);
+        bigy = __syncthreads_or(big & 2);
     }
-    const bool bigx = __syncthreads_or(big & 1), bigy = __syncthreads_or(big & 2);
     if ((!bigx || !bigy) && d_first < nb) {
         const uint32_t sides = (bigx ? 0u : 1u) | (bigy ? 0u : 2u);
         for (uint32_t t = d_first + threadIdx.x; t < 2 * nb; t += blockDim.x) {
