@@ -39,6 +39,8 @@ constexpr uint32_t kSmallPassBits = 8;          // sort-merge: one pass up to 2^
 constexpr uint32_t kMaxUnitPages = 2048;        // pass-2 work unit: <= 128K tuples
 constexpr uint32_t kMinUnitPages = kPTile / 64;  // one tile
 constexpr uint32_t kNone = 0xFFFFFFFFu;
+constexpr uint32_t kHotRun = kPTile / 2;        // a digit above this many tuples of a tile is hot
+constexpr uint32_t kHotWord = 40;               // misc[] word of the hot digit
 
 // Pages written by one pass for one relation.
 struct PageSet {
@@ -187,7 +189,8 @@ partition_pass(PassArgs a) {
     uint32_t *b2 = b1 + F;
     uint32_t *npos = b2 + F;
     uint32_t *misc = npos + F;          // [0] pool pages taken, [1] tuples in the tile,
-                                        // [8..24) per-warp totals of the digit scan
+                                        // [8..24) per-warp totals of the digit scan,
+                                        // [kHotWord] hot digit
     uint32_t *upage = misc + 48;        // paged input: this unit's pages
     uint8_t *ucnt = reinterpret_cast<uint8_t *>(upage + kMaxUnitPages);
 
@@ -202,7 +205,10 @@ partition_pass(PassArgs a) {
         cnt[F + d] = 0;
         npos[d] = kNone;
     }
-    if (tid == 0) misc[0] = 0;
+    if (tid == 0) {
+        misc[0] = 0;
+        misc[kHotWord] = kNone;
+    }
     if (kPaged)
         for (uint64_t i = b + tid; i < e; i += kThreads) {
             const uint32_t pg = in.plist[i];
@@ -289,12 +295,38 @@ partition_pass(PassArgs a) {
     uint32_t par = 0;
     for (uint64_t t0 = b; t0 < e; t0 += kStep, par ^= F) {
         uint32_t *c = cnt + par;
-        // A. rank each tuple within its digit
+        // A. rank each tuple within its digit.  A digit that held more than
+        //    half of the previous tile (a hot key under skew) takes its ranks
+        //    from one atomic per warp and tuple slot, by ballot: its increments
+        //    would otherwise serialise on one shared counter.
         uint32_t rk[kPer / 2];   // two 16-bit ranks per word
+        const uint32_t hot = misc[kHotWord];   // block-uniform
+        if (hot == kNone) {
 #pragma unroll
-        for (int k = 0; k < kPer; k++) {
-            const uint32_t r = (valid >> k) & 1 ? atomicAdd(&c[df(tkey(w[k]))], 1u) : 0u;
-            if (k & 1) rk[k / 2] |= r << 16; else rk[k / 2] = r;
+            for (int k = 0; k < kPer; k++) {
+                const uint32_t r = (valid >> k) & 1 ? atomicAdd(&c[df(tkey(w[k]))], 1u) : 0u;
+                if (k & 1) rk[k / 2] |= r << 16; else rk[k / 2] = r;
+            }
+        } else {
+            uint32_t lt;
+            asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
+#pragma unroll
+            for (int k = 0; k < kPer; k++) {
+                const bool ok = (valid >> k) & 1;
+                const uint32_t d = ok ? df(tkey(w[k])) : kNone;
+                const uint32_t m = __ballot_sync(0xffffffffu, d == hot);
+                uint32_t r = 0;
+                if (d == hot) r = (uint32_t)__popc(m & lt);
+                else if (ok) r = atomicAdd(&c[d], 1u);
+                if (m) {   // warp-uniform
+                    const int leader = __ffs(m) - 1;
+                    uint32_t base = 0;
+                    if (lane == leader) base = atomicAdd(&c[hot], (uint32_t)__popc(m));
+                    base = __shfl_sync(0xffffffffu, base, leader);
+                    if (d == hot) r += base;
+                }
+                if (k & 1) rk[k / 2] |= r << 16; else rk[k / 2] = r;
+            }
         }
         __syncthreads();
         // B. digit runs of the tile, pages, stream positions.  Up to 32 digits
@@ -359,17 +391,20 @@ partition_pass(PassArgs a) {
                         first += pages_for(Ls[j], Ps[j]);
                     }
                 }
+                // the largest run (one digit per lane here): the next tile's hot digit
+                const uint32_t mx = __reduce_max_sync(0xffffffffu, (Ls[0] << 16) | (uint32_t)lane);
                 __syncwarp();
                 if (lane == 0) {
                     misc[0] = pool0 + (all >> 16);
                     misc[1] = all & 0xFFFFu;
+                    misc[kHotWord] = (mx >> 16) > kHotRun ? (mx & 0xFFFFu) : kNone;
                 }
             }
         } else {
             const uint32_t nbw = (F + 31) / 32;                 // B warps
             const int bw = tid >> 5;
             const uint32_t d = (uint32_t)tid;                   // this lane's digit
-            uint32_t L = 0, p = kNone, need = 0, inc = 0, pool0 = 0;
+            uint32_t L = 0, p = kNone, need = 0, inc = 0, pool0 = 0, mx = 0;
             if (bw < (int)nbw) {
                 if (d < F) {
                     L = c[d];
@@ -377,8 +412,10 @@ partition_pass(PassArgs a) {
                     need = pages_for(L, p);
                 }
                 inc = warp_incl_scan(L | (need << 16), lane);   // L <= kPTile, pages of 32 digits < 2^16
+                mx = __reduce_max_sync(0xffffffffu, (L << 16) | d);   // this warp's largest run, its digit
                 pool0 = misc[0];
                 if (lane == 31) misc[8 + bw] = inc;
+                if (tid == 0) misc[kHotWord] = kNone;   // all of this tile's readers are past step A
             }
             __syncthreads();   // every B warp has read misc[0] and written its total
             if (bw < (int)nbw) {
@@ -396,6 +433,8 @@ partition_pass(PassArgs a) {
                     misc[0] = pool0 + all_p;
                     misc[1] = all_t;
                 }
+                // the next tile's hot digit: a run above half a tile (at most one)
+                if (lane == 0 && (mx >> 16) > kHotRun) misc[kHotWord] = mx & 0xFFFFu;
             }
         }
         __syncthreads();
