@@ -15,6 +15,7 @@ namespace adb {
 
 constexpr int kNumSMs = 148;          // B200: 2 dies x 74 SMs
 constexpr int kWarp = 32;
+constexpr uint32_t kFibMul = 0x9E3779B1u;   // 2^32 / golden ratio: Fibonacci hashing (Knuth, TAOCP 6.4)
 
 __host__ __device__ __forceinline__ uint32_t tkey(uint64_t w) { return (uint32_t)(w >> 32); }
 __host__ __device__ __forceinline__ uint32_t tpay(uint64_t w) { return (uint32_t)w; }

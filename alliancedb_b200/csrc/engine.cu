@@ -318,7 +318,7 @@ static size_t scratch_for(const AlgoEntry *a, uint64_t nR, uint64_t nS, const ad
         case Family::Radix:
         case Family::RadixHist:
             return radix_scratch(nR, nS, radix_bits_for(nR, p ? p->radix_bits : 0), num_sms);
-        case Family::Npo: return npo_scratch(nR);
+        case Family::Npo: return npo_scratch(nR, nS, p ? p->radix_bits : 0, num_sms);
         case Family::SortMerge: return smj_scratch(nR, nS, p ? p->part_fanout : 0, num_sms);
         case Family::Shj:
         case Family::Pmj:
@@ -335,7 +335,7 @@ static int dispatch(Context *ctx, const AlgoEntry *a, const DevJoin &j, const ad
             return run_radix(ctx, j, false, radix_bits_for(j.nR, p ? p->radix_bits : 0), acc);
         case Family::RadixHist:
             return run_radix(ctx, j, true, radix_bits_for(j.nR, p ? p->radix_bits : 0), acc);
-        case Family::Npo: return run_npo(ctx, j, acc);
+        case Family::Npo: return run_npo(ctx, j, p ? p->radix_bits : 0, acc);
         case Family::SortMerge: return run_smj(ctx, j, p ? p->part_fanout : 0, a->model == 1, acc);
         case Family::Shj:
         case Family::Pmj:

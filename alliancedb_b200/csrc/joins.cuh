@@ -39,8 +39,9 @@ size_t radix_scratch(uint64_t nR, uint64_t nS, int bits, int num_sms);
 int run_radix(Context *ctx, const DevJoin &j, bool hist_table, int bits, unsigned long long *acc);
 
 // ---- NPO / NPO_st ----
-size_t npo_scratch(uint64_t nR);
-int run_npo(Context *ctx, const DevJoin &j, unsigned long long *acc);
+uint32_t npo_region_bits(uint64_t nR, int requested);
+size_t npo_scratch(uint64_t nR, uint64_t nS, int region_bits, int num_sms);
+int run_npo(Context *ctx, const DevJoin &j, int region_bits, unsigned long long *acc);
 
 // ---- m-way / m-pass ----
 size_t smj_scratch(uint64_t nR, uint64_t nS, int part_fanout, int num_sms);

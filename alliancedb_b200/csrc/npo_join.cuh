@@ -23,7 +23,19 @@ constexpr uint64_t kEmpty = ~0ULL;
 
 __host__ __device__ __forceinline__ uint32_t npo_hash(uint32_t key, uint32_t log2n) {
     // Fibonacci hashing: the top log2n bits of key * 2^32/phi
-    return log2n ? (uint32_t)((key * 0x9E3779B1u) >> (32 - log2n)) : 0u;
+    return log2n ? (uint32_t)((key * kFibMul) >> (32 - log2n)) : 0u;
+}
+
+// Inserts tuple word w (not the empty marker) by linear probing from `slot`.
+__device__ __forceinline__ void npo_insert_from(uint64_t *table, uint64_t mask, uint64_t slot, uint64_t w,
+                                                int *err) {
+    for (uint64_t tries = 0;;) {
+        const unsigned long long prev = atomicCAS(reinterpret_cast<unsigned long long *>(table + slot),
+                                                  (unsigned long long)kEmpty, (unsigned long long)w);
+        if (prev == kEmpty) return;
+        slot = (slot + 1) & mask;
+        if (++tries > mask) { atomicExch(err, 2); return; }   // table full: cannot happen at load <= 0.5
+    }
 }
 
 // static: each translation unit that includes this header gets its own copy
@@ -34,24 +46,77 @@ static __global__ void npo_build(const uint64_t *__restrict__ R, uint64_t nR, ui
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nR; i += stride) {
         const uint64_t w = R[i];
         if (w == kEmpty) { atomicAdd(sentinel_cnt, 1ull); continue; }
-        uint64_t slot = npo_hash(tkey(w), log2n);
-        uint64_t tries = 0;
-        while (true) {
-            const unsigned long long prev =
-                atomicCAS(reinterpret_cast<unsigned long long *>(table + slot), (unsigned long long)kEmpty,
-                          (unsigned long long)w);
-            if (prev == kEmpty) break;
-            slot = (slot + 1) & mask;
-            if (++tries > mask) { atomicExch(err, 2); break; }   // table full: cannot happen at load <= 0.5
+        npo_insert_from(table, mask, npo_hash(tkey(w), log2n), w, err);
+    }
+}
+
+// Count, checksum and optional materialisation of a probe's matches.
+template <bool kMaterialize>
+struct NpoSink {
+    Acc a;
+    uint64_t *mat;
+    unsigned long long *mat_n;
+    uint64_t mat_cap;
+    __device__ __forceinline__ void match(uint64_t s, uint32_t key, uint32_t rpay, uint64_t sh) {
+        a.count++;
+        a.sum += pair_hash_pre(key, rpay, sh);
+        if (kMaterialize) {
+            const unsigned long long k = atomicAdd(mat_n, 1ull);
+            if (k < mat_cap) mat[k] = s;
         }
+    }
+};
+
+// One probe: S tuple s with start slot `slot`, given the 32-byte sector that
+// holds the start slot (lo, hi).  The sector is scanned from the start slot;
+// only a probe whose run of occupied slots reaches the sector's end goes on
+// slot by slot, as linear probing does.  nsent = build tuples equal to the
+// empty marker (they match key 0xFFFFFFFF).
+template <bool kMaterialize>
+__device__ __forceinline__ void npo_probe_one(NpoSink<kMaterialize> &sink, const uint64_t *table, uint64_t mask,
+                                              uint64_t s, uint64_t slot, ulonglong2 lo, ulonglong2 hi,
+                                              uint64_t nsent) {
+    const uint32_t key = tkey(s);
+    const uint64_t sh = s_half(key, tpay(s));
+    const uint64_t w4[4] = {lo.x, lo.y, hi.x, hi.y};
+    bool open = true;   // no empty slot met yet
+    uint32_t hits = 0;  // matching slots of the sector
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        if (open && (uint64_t)j >= (slot & 3)) {
+            if (w4[j] == kEmpty) open = false;
+            else if (tkey(w4[j]) == key) hits |= 1u << j;
+        }
+    }
+    while (hits) {       // one call site for the checksum (usually one match)
+        const int j = __ffs(hits) - 1;
+        hits &= hits - 1;
+        const ulonglong2 h2 = j & 2 ? hi : lo;
+        sink.match(s, key, tpay(j & 1 ? h2.y : h2.x), sh);
+    }
+    if (open) {   // the run reaches the sector's end: continue linear probing
+        uint64_t sl = ((slot & ~3ULL) + 4) & mask;
+        for (uint64_t tries = 0; tries <= mask; tries++) {
+            const uint64_t v = table[sl];
+            if (v == kEmpty) break;
+            if (tkey(v) == key) sink.match(s, key, tpay(v), sh);
+            sl = (sl + 1) & mask;
+        }
+    }
+    if (key == 0xFFFFFFFFu && nsent) {
+        sink.a.count += nsent;
+        sink.a.sum += nsent * pair_hash_pre(key, 0xFFFFFFFFu, sh);
+        if (kMaterialize)
+            for (uint64_t t = 0; t < nsent; t++) {
+                const unsigned long long k = atomicAdd(sink.mat_n, 1ull);
+                if (k < sink.mat_cap) sink.mat[k] = s;
+            }
     }
 }
 
 // Probe: each thread takes kProbeU S tuples at a time (a grid-stride group),
-// so that kProbeU random table reads are in flight per thread.  A probe reads
-// the whole 32-byte sector that holds its start slot (two 16-byte loads) and
-// scans it from the start slot; only a probe whose run of occupied slots
-// reaches the sector's end goes on slot by slot, as linear probing does.
+// so that kProbeU random table reads are in flight per thread; a probe reads
+// the whole 32-byte sector that holds its start slot (two 16-byte loads).
 constexpr int kProbeU = 4;
 
 template <bool kMaterialize>
@@ -63,15 +128,7 @@ __global__ void npo_probe(const uint64_t *__restrict__ S, uint64_t nS, const uin
     const uint64_t T = (uint64_t)gridDim.x * blockDim.x;
     const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t nsent = *sentinel_cnt;
-    Acc a;
-    auto match = [&](uint64_t s, uint32_t key, uint32_t rpay, uint64_t sh) {
-        a.count++;
-        a.sum += pair_hash_pre(key, rpay, sh);
-        if (kMaterialize) {
-            const unsigned long long k = atomicAdd(mat_n, 1ull);
-            if (k < mat_cap) mat[k] = s;
-        }
-    };
+    NpoSink<kMaterialize> sink{Acc(), mat, mat_n, mat_cap};
     for (uint64_t g0 = tid; g0 < nS; g0 += T * kProbeU) {
         uint64_t s[kProbeU], slot[kProbeU];
         ulonglong2 lo[kProbeU], hi[kProbeU];
@@ -92,47 +149,10 @@ __global__ void npo_probe(const uint64_t *__restrict__ S, uint64_t nS, const uin
             }
         }
 #pragma unroll
-        for (int u = 0; u < kProbeU; u++) {
-            if (!ok[u]) continue;
-            const uint32_t key = tkey(s[u]);
-            const uint64_t sh = s_half(key, tpay(s[u]));
-            const uint64_t w4[4] = {lo[u].x, lo[u].y, hi[u].x, hi[u].y};
-            bool open = true;   // no empty slot met yet
-            uint32_t hits = 0;  // matching slots of the sector
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                if (open && (uint64_t)j >= (slot[u] & 3)) {
-                    if (w4[j] == kEmpty) open = false;
-                    else if (tkey(w4[j]) == key) hits |= 1u << j;
-                }
-            }
-            while (hits) {       // one call site for the checksum (usually one match)
-                const int j = __ffs(hits) - 1;
-                hits &= hits - 1;
-                const ulonglong2 h2 = j & 2 ? hi[u] : lo[u];
-                match(s[u], key, tpay(j & 1 ? h2.y : h2.x), sh);
-            }
-            if (open) {   // the run reaches the sector's end: continue linear probing
-                uint64_t sl = ((slot[u] & ~3ULL) + 4) & mask;
-                for (uint64_t tries = 0; tries <= mask; tries++) {
-                    const uint64_t v = table[sl];
-                    if (v == kEmpty) break;
-                    if (tkey(v) == key) match(s[u], key, tpay(v), sh);
-                    sl = (sl + 1) & mask;
-                }
-            }
-            if (key == 0xFFFFFFFFu && nsent) {
-                a.count += nsent;
-                a.sum += nsent * pair_hash_pre(key, 0xFFFFFFFFu, sh);
-                if (kMaterialize)
-                    for (uint64_t t = 0; t < nsent; t++) {
-                        const unsigned long long k = atomicAdd(mat_n, 1ull);
-                        if (k < mat_cap) mat[k] = s[u];
-                    }
-            }
-        }
+        for (int u = 0; u < kProbeU; u++)
+            if (ok[u]) npo_probe_one(sink, table, mask, s[u], slot[u], lo[u], hi[u], nsent);
     }
-    block_flush(a, acc, red);
+    block_flush(sink.a, acc, red);
 }
 
 }  // namespace adb

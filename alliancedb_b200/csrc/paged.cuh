@@ -144,8 +144,9 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x, int lane) {
 // completed by the neighbouring tiles of the same stream while the line is
 // still in L2.  Three barriers per tile (four above 32 digits); the next
 // tile's loads are in flight during D.  kMode: 0 flat input, 1 paged input
-// (pass 2), 2 segmented flat input (batched windows).
-template <int kMode, int kThreads>
+// (pass 2), 2 segmented flat input (batched windows).  kHashed: the digit is
+// taken from key * kFibMul instead of the key (the table regions of NPO).
+template <int kMode, int kThreads, bool kHashed = false>
 __global__ void __launch_bounds__(kThreads, kPassMinBlocks)
 partition_pass(PassArgs a) {
     constexpr bool kPaged = kMode == 1;
@@ -181,6 +182,7 @@ partition_pass(PassArgs a) {
         }
     }
     const uint32_t F = df.mask + 1;
+    auto dig = [&](uint64_t w) { return df(kHashed ? tkey(w) * kFibMul : tkey(w)); };
     uint64_t *stage = reinterpret_cast<uint64_t *>(smem);
     uint32_t *cnt = reinterpret_cast<uint32_t *>(stage + kPTile);   // [2][F]
     uint32_t *toff = cnt + 2 * F;
@@ -304,7 +306,7 @@ partition_pass(PassArgs a) {
         if (hot == kNone) {
 #pragma unroll
             for (int k = 0; k < kPer; k++) {
-                const uint32_t r = (valid >> k) & 1 ? atomicAdd(&c[df(tkey(w[k]))], 1u) : 0u;
+                const uint32_t r = (valid >> k) & 1 ? atomicAdd(&c[dig(w[k])], 1u) : 0u;
                 if (k & 1) rk[k / 2] |= r << 16; else rk[k / 2] = r;
             }
         } else {
@@ -313,7 +315,7 @@ partition_pass(PassArgs a) {
 #pragma unroll
             for (int k = 0; k < kPer; k++) {
                 const bool ok = (valid >> k) & 1;
-                const uint32_t d = ok ? df(tkey(w[k])) : kNone;
+                const uint32_t d = ok ? dig(w[k]) : kNone;
                 const uint32_t m = __ballot_sync(0xffffffffu, d == hot);
                 uint32_t r = 0;
                 if (d == hot) r = (uint32_t)__popc(m & lt);
@@ -442,7 +444,7 @@ partition_pass(PassArgs a) {
 #pragma unroll
         for (int k = 0; k < kPer; k++)
             if ((valid >> k) & 1)
-                stage[toff[df(tkey(w[k]))] + ((rk[k / 2] >> ((k & 1) * 16)) & 0xFFFFu)] = w[k];
+                stage[toff[dig(w[k])] + ((rk[k / 2] >> ((k & 1) * 16)) & 0xFFFFu)] = w[k];
         const uint32_t tile_n = misc[1];
         if (t0 + kStep < e) {   // in flight during D; the tile after that into L2
             prefetch_tile(t0 + 2 * kStep);
@@ -452,7 +454,7 @@ partition_pass(PassArgs a) {
         // D. stage slots to their pages
         for (uint32_t i = tid; i < tile_n; i += kThreads) {
             const uint64_t v = stage[i];
-            const uint32_t d = df(tkey(v));
+            const uint32_t d = dig(v);
             const uint32_t dst = i + (i < lim[d] ? b1[d] : b2[d]);
             o.pages[dst] = v;
             if ((dst & (kPageTuples - 1)) == 0) {   // first slot of a page taken in B

@@ -24,6 +24,7 @@ __device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
 struct DigitFn {
     uint32_t shift;
     uint32_t mask;      // F - 1
+    bool hashed = false;   // the pass applies it to key * kFibMul (flat passes only)
     __host__ __device__ __forceinline__ uint32_t operator()(uint32_t key) const { return (key >> shift) & mask; }
 };
 

@@ -31,6 +31,7 @@ static void launch_pass(const PassArgs &a, uint32_t F, int G, bool paged, cudaSt
     const dim3 grid(G, 2);
     const size_t smem = pass_smem(F, paged);
     if (paged) partition_pass<1, kPassThreads><<<grid, kPassThreads, smem, st>>>(a);
+    else if (a.df.hashed) partition_pass<0, kPassThreads, true><<<grid, kPassThreads, smem, st>>>(a);
     else partition_pass<0, kPassThreads><<<grid, kPassThreads, smem, st>>>(a);
 }
 
@@ -278,6 +279,8 @@ int run_radix(Context *ctx, const DevJoin &j, bool hist_table, int bits, unsigne
 int radix_set_attrs() {
     ADB_CK(cudaFuncSetAttribute(partition_pass<0, kPassThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)pass_smem(1u << kMaxPassBits, false)));
+    ADB_CK(cudaFuncSetAttribute(partition_pass<0, kPassThreads, true>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pass_smem(1u << kMaxPassBits, false)));
     ADB_CK(cudaFuncSetAttribute(partition_pass<1, kPassThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)pass_smem(1u << kMaxPassBits, true)));
     ADB_CK(cudaFuncSetAttribute(radix_join_items<TableKind::Chain>,

@@ -75,7 +75,9 @@ typedef struct adb_join_params {
     int32_t group_size;         /* param_t.group_size, JBCR groups (-G) */
     int32_t progressive_step;   /* param_t.progressive_step, PMJ run size in % of each side */
     int32_t merge_step;         /* param_t.merge_step, PMJ runs merged per step */
-    int32_t radix_bits;         /* PRO/PRH/RJ fan-out bits; 0 = chosen from |R| */
+    int32_t radix_bits;         /* PRO/PRH/RJ fan-out bits; 0 = chosen from |R|.  NPO: bits of the table
+                                   regions its inputs are grouped by (up to 9); 0 = chosen from |R|
+                                   (none while the table fits in L2), < 0 = no grouping */
     int32_t part_fanout;        /* joinconfig_t.PARTFANOUT for m-way/m-pass; 0 = chosen */
     int32_t materialize;        /* 1: also write <S-key, S-payload> per match (JOIN_RESULT_MATERIALIZE) */
     int32_t batch_tuples;       /* eager joins: arrival micro-batch in tuples per side; 0 = 1 ms of stream */
@@ -97,7 +99,8 @@ typedef struct adb_join_result {
     int32_t kernels;            /* kernels this call launched */
     float ms_device;            /* device time of the join, CUDA events on the library stream */
     float ms_phase[4];          /* device time per phase; radix: partition pass 1, pass 2 (0 with one pass),
-                                   work list, join kernel; NPO: build, -, -, probe; m-way: partitioning,
+                                   work list, join kernel; NPO: grouping by table region, build, -, probe;
+                                   m-way: partitioning,
                                    work list, -, sort + merge-join kernel */
     float ms_h2d;               /* host->device copy time (adb_join only) */
     uint64_t materialized;      /* tuples written to the materialisation buffer */
