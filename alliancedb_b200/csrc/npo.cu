@@ -4,9 +4,9 @@
 // probe S chunks).
 //
 // The table is one global open-addressing array of 2^l2 slots (npo_join.cuh),
-// as the reference's is one shared bucket array.  Up to 64 MB it stays in L2
-// and the join is: clear the table, one build launch, one probe launch over
-// the relations as they are.
+// as the reference's is one shared bucket array.  Up to 256 MB (|R| <= 2^24)
+// the join is: clear the table, one build launch, one probe launch over the
+// relations as they are.
 //
 // A larger table (8 B x 2 |R|: 2 GiB at |R| = 2^27) is 16x the L2, and build
 // and probe in input order would each touch a random DRAM sector per tuple.
@@ -35,15 +35,21 @@ static uint32_t npo_log2(uint64_t nR) {
 }
 
 constexpr uint32_t kNpoRegionLog2 = 21;     // slots per table region (16 MB)
-constexpr uint32_t kNpoL2ResidentLog2 = 23; // tables up to 2^23 slots (64 MB) are not grouped
+// Tables up to 2^25 slots (256 MB) are not grouped.  Measured (whole join,
+// |R| = |S|, grouped / not): 2^23 0.66 / 0.58 ms, 2^24 2.08 / 1.47 ms,
+// 2^25 1.25 / 2.45 ms, 2^26 2.48 / 5.28 ms, 2^27 4.80 / 10.9 ms.  The grouped
+// build runs at 68-69 G inserts/s from 2^25 up but at 11-23 G/s at 2^23 and
+// 2^24 (tables of 1-2x the L2), whatever the region size; the cause is not
+// known.
+constexpr uint32_t kNpoUngroupedLog2 = 25;
 
-// Table-region bits: 0 (no grouping) while the table fits in L2, else regions
-// of 2^21 slots.  requested > 0 forces that many bits, < 0 no grouping; at
+// Table-region bits: 0 (no grouping) up to a 256 MB table, else regions of
+// 2^21 slots.  requested > 0 forces that many bits, < 0 no grouping; at
 // most 2^9 regions (one partition pass) of at least 16 slots (one L2 line).
 uint32_t npo_region_bits(uint64_t nR, int requested) {
     const uint32_t l2 = npo_log2(nR);
     if (requested < 0) return 0;
-    int rb = requested > 0 ? requested : (l2 > kNpoL2ResidentLog2 ? (int)(l2 - kNpoRegionLog2) : 0);
+    int rb = requested > 0 ? requested : (l2 > kNpoUngroupedLog2 ? (int)(l2 - kNpoRegionLog2) : 0);
     if (rb > (int)kMaxPassBits) rb = (int)kMaxPassBits;
     if (rb > (int)l2 - 4) rb = (int)l2 - 4;
     return rb < 0 ? 0u : (uint32_t)rb;

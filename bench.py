@@ -53,15 +53,17 @@ ALG_BYTES = {"PRO": 24, "RJ_st": 24, "PRH": 24, "PRHO": 24, "NPO": 16, "NPO_st":
 # Per family: phase index (adb_join_result.ms_phase) -> (kernel, algorithmic
 # bytes per input tuple of one launch, DRAM bytes per input tuple of one launch
 # from an ncu capture of dram__bytes_read.sum + dram__bytes_write.sum at
-# |R| = |S| = 2^24, None where not captured).  The traffic of a full-size
+# |R| = |S| = 2^24, for NPO at 2^25, the smallest size it groups by table
+# region; None where not captured).  The traffic of a full-size
 # launch is that figure times the launch's tuples: the kernels stream every
 # tuple once, so traffic grows in proportion.
 KERNELS = {
-    "radix": {0: ("partition_pass<0,512> (pass 1)", 16, (270269696 + 214559744) / 2**25),
-              1: ("partition_pass<1,512> (pass 2)", 16, (276501504 + 214193152) / 2**25),
-              3: ("radix_join_items<Chain>", 8, (273603584 + 3484416) / 2**25)},
-    "npo": {0: ("partition_pass<0,512,hashed> (grouping by table region)", 16, None),
-            1: ("npo_build_pages", 8, None), 3: ("npo_probe_pages", 8, None)},
+    "radix": {0: ("partition_pass<0,512> (pass 1)", 16, (270247168 + 213934080) / 2**25),
+              1: ("partition_pass<1,512> (pass 2)", 16, (276288768 + 214363648) / 2**25),
+              3: ("radix_join_items<Chain>", 8, (273622272 + 3668736) / 2**25)},
+    "npo": {0: ("partition_pass<0,512,hashed> (grouping by table region)", 16, (540667392 + 486182144) / 2**26),
+            1: ("npo_build_pages", 8, (812259584 + 381960960) / 2**26),
+            3: ("npo_probe_pages", 8, (967028736 + 4030976) / 2**26)},
     "smj": {0: ("partition_pass (both passes)", 32,
                 (271074048 + 215111680 + 279591680 + 219554048) / 2**25),
             3: ("smj_items", 8, (281787648 + 3820288) / 2**25)},
@@ -518,7 +520,7 @@ def main():
                      "frac": achieved / hbm, "peak_source": peak_kind,
                      "alg_bytes_per_launch": dom_bytes, "kernel_ms": float(ph[dom]),
                      "traffic": traffic, "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum "
-                                                           "per tuple at |R|=|S|=2^24, scaled to this launch"
+                                                           "per tuple at |R|=|S|=2^24 (NPO 2^25), scaled to this launch"
                                                            if traffic else None,
                      "pipeline": {"alg_bytes_per_tuple": ALG_BYTES.get(args.algo, 24), "achieved": pipe_gbs,
                                   "frac": pipe_gbs / hbm}},

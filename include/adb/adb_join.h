@@ -77,7 +77,7 @@ typedef struct adb_join_params {
     int32_t merge_step;         /* param_t.merge_step, PMJ runs merged per step */
     int32_t radix_bits;         /* PRO/PRH/RJ fan-out bits; 0 = chosen from |R|.  NPO: bits of the table
                                    regions its inputs are grouped by (up to 9); 0 = chosen from |R|
-                                   (none while the table fits in L2), < 0 = no grouping */
+                                   (none up to a 256 MB table, |R| <= 2^24), < 0 = no grouping */
     int32_t part_fanout;        /* joinconfig_t.PARTFANOUT for m-way/m-pass; 0 = chosen */
     int32_t materialize;        /* 1: also write <S-key, S-payload> per match (JOIN_RESULT_MATERIALIZE) */
     int32_t batch_tuples;       /* eager joins: arrival micro-batch in tuples per side; 0 = 1 ms of stream */

@@ -1,6 +1,6 @@
 """NPO with its inputs grouped by table region, on the B200.
 
-Above a 64 MB table (|R| > 2^22) NPO groups R and S by the top bits of the
+Above a 256 MB table (|R| > 2^24) NPO groups R and S by the top bits of the
 hash (the table region of each key) with one partition pass, then builds and
 probes in region order so that the region being worked on stays in L2.  The
 table is the same single open-addressing array; only the order of inserts and
@@ -104,8 +104,8 @@ def test_grouped_materialization(oracle):
 
 
 def test_automatic_grouping_above_l2(oracle):
-    """|R| = 2^23: a 128 MB table, grouped into 8 regions by default; phase 0 is the grouping pass."""
-    R = adb.gen_pk(1 << 23, 33)
+    """|R| = 2^25: a 512 MB table, grouped into 32 regions by default; phase 0 is the grouping pass."""
+    R = adb.gen_pk(1 << 25, 33)
     S = adb.gen_fk(1 << 23, R, 0.7, 34)
     truth = oracle.pk_truth(R, S)
     got = adb.join("NPO", R, S)
