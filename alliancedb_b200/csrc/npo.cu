@@ -20,7 +20,7 @@
 // region g also prefetches its share of region g + 1's table lines into L2,
 // so the next region arrives by line reads instead of random sector misses.
 // At |R| = |S| = 2^27 this takes NPO from 10.9 ms (build 6.94, probe 3.89)
-// to about 4.8 ms (grouping 1.06, build 1.98, probe 1.75).
+// to 4.26 ms (grouping 1.06, build 1.95, probe 1.19).
 // Matches, count and checksum are the same as in input order.
 #include "joins.cuh"
 #include "npo_join.cuh"
@@ -28,7 +28,7 @@
 
 namespace adb {
 
-// 2 slots per build tuple, at least 4 (one 32-byte sector: the probe reads whole sectors)
+// 2 slots per build tuple, at least 4 (the probe's first read is a four-slot window)
 static uint32_t npo_log2(uint64_t nR) {
     uint32_t l = ceil_log2_u64(2 * (nR ? nR : 1));
     return l < 2 ? 2 : l;
@@ -156,10 +156,10 @@ npo_build_pages(NpoPages P, uint64_t *__restrict__ table, uint32_t log2n, uint32
 }
 
 // Probe over S's pages in region order: one warp per pair of adjacent pages,
-// four probes (sector loads) in flight per lane.  No prefetch here: the
-// region's lines come in by the probes' own reads (at |S| = 2^27, 1.75 ms
-// without the next-region prefetch, 2.26 ms with it, 2.53 ms with loads two
-// regions ahead).
+// four probes (window loads) in flight per lane.  No prefetch here: the
+// region's lines come in by the probes' own reads (at |S| = 2^27, with the
+// sector-first probe: 1.75 ms without the next-region prefetch, 2.26 ms with
+// it, 2.53 ms with loads two regions ahead).
 template <bool kMaterialize>
 __global__ void __launch_bounds__(kNpoThreads, 4)
 npo_probe_pages(NpoPages P, const uint64_t *__restrict__ table, uint32_t log2n,
@@ -193,13 +193,9 @@ npo_probe_pages(NpoPages P, const uint64_t *__restrict__ table, uint32_t log2n,
             }
         }
 #pragma unroll
-        for (int u = 0; u < 4; u++) {   // the sectors: all loads issued before any is used
+        for (int u = 0; u < 4; u++) {   // the windows: all loads issued before any is used
             slot[u] = npo_hash(tkey(s[u]), log2n);
-            const ulonglong2 *sec = reinterpret_cast<const ulonglong2 *>(table + (slot[u] & ~3ULL));
-            if (ok[u]) {
-                lo[u] = __ldg(sec);
-                hi[u] = __ldg(sec + 1);
-            }
+            if (ok[u]) npo_window(table, mask, slot[u], lo[u], hi[u]);
         }
 #pragma unroll
         for (int u = 0; u < 4; u++)

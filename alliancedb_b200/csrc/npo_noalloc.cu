@@ -104,7 +104,7 @@ extern "C" int adb_npo_join_noalloc(const adb_tuple *dR, uint64_t nR, const adb_
     ADB_TRY(noalloc_scratch_ptr(&scratch));
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     uint32_t l2 = ceil_log2_u64(2 * (nR ? nR : 1));
-    if (l2 < 2) l2 = 2;   // at least one 32-byte sector (the probe reads whole sectors)
+    if (l2 < 2) l2 = 2;   // at least four slots (the probe's first read is a four-slot window)
     uint64_t *table = reinterpret_cast<uint64_t *>(scratch);
     unsigned long long *acc = scratch + kNoAllocTableSlots;   // count, checksum, err, sentinel
     ADB_CK(cudaMemsetAsync(table, 0xFF, (1ULL << l2) * sizeof(uint64_t), st));
