@@ -13,9 +13,11 @@
 //      keys meet in one partition, as the reference's range partition
 //      guarantees for its key ranges;
 //   2. smj_items, a persistent work-stealing kernel: per work item it copies an
-//      R chunk (<= 4096 tuples) into shared memory with bulk async copies, sorts
-//      it, loads and sorts the item's S block, and merge-joins the two sorted
-//      runs with merge-path partitioning across the CTA's threads.
+//      R chunk (<= 4096 tuples) and the item's S block into shared memory with
+//      bulk async copies, sorts R, and joins S bucket by bucket against R's
+//      sorted buckets (S is bucketed by the same key bits, not moved); only
+//      keys 0xFFFFFFFF, or an R chunk that needed the bitonic fallback, sort S
+//      as well and merge the two sorted runs with merge-path partitioning.
 // The per-chunk sort is an MSD counting sort on the (at most) 11 highest key
 // bits that differ within the chunk, followed by an insertion sort inside
 // each bucket: the bits above those are equal across the chunk, so the result
@@ -70,7 +72,8 @@ struct SmjRec {
     uint32_t pad_;
 };
 
-static_assert(16 + 8 * 96 + 2 * sizeof(SmjRec) <= 1024, "barrier, scratch and records exceed the tail");
+static_assert(16 + 8 * 112 + 2 * sizeof(SmjRec) <= 1024 && kDualRedWords <= 224,
+              "barrier, scratch and records exceed the tail");
 
 // Items are pipelined as in radix_join_items: while item i is merge-joined by
 // warps 0 .. 30, the last warp builds the page table of item i + 1 and takes
@@ -84,8 +87,8 @@ smj_items(SmjArgs a) {
     uint32_t *cnt = reinterpret_cast<uint32_t *>(C + kSmjCap);
     uint32_t *ptab = cnt + kDualCntWords;                    // [2] x {pg[kSmjTabEntries], dst << 8 | count []}
     uint64_t *bar = reinterpret_cast<uint64_t *>(ptab + 4 * kSmjTabEntries);
-    uint64_t *red = bar + 2;                                 // 96 u64 (192 u32 of sort scratch)
-    SmjRec *rec = reinterpret_cast<SmjRec *>(red + 96);      // [2]
+    uint64_t *red = bar + 2;                                 // 112 u64 (224 u32 of sort scratch)
+    SmjRec *rec = reinterpret_cast<SmjRec *>(red + 112);     // [2]
     __shared__ uint32_t runn[2];   // length of R's run of a single S key, per item parity
 
     const uint32_t n_items = *a.n_items;
@@ -207,12 +210,20 @@ smj_items(SmjArgs a) {
         // words visible to it: no block barrier before the analysis
         if (!mbar_wait(bar, phase) || a.waits_run_out) atomicExch(a.err, 1);
         phase ^= 1;
-        // sorted R (+ pads) in B, sorted S (+ pads) in A; the pads are the last
-        // words of each run and a real all-ones tuple is the same word, so
-        // dropping as many words as there are pads is exact.  An S block of one
-        // key K is not sorted, and neither is R: R's run of K is gathered into B.
+        // sorted R (+ pads) in B; sorted S (+ pads) in A where the merge path
+        // needs it, else S stays in C and is only bucketed.  The pads are the
+        // last words of each sorted run and a real all-ones tuple is the same
+        // word, so dropping as many words as there are pads is exact.  An S
+        // block of one key K is not sorted, and neither is R: R's run of K is
+        // gathered into B.
         uint32_t *red32 = reinterpret_cast<uint32_t *>(red);
         DualSort ds = dual_analyze(A, rslots, C, sslots, cnt, red32, spad);
+        // all-ones words beyond the pads: real tuples with key 0xFFFFFFFF
+        const bool ones = ds.onesx != rpad || ds.onesy != spad;
+        // the S block needs an order only for the merge path (keys 0xFFFFFFFF);
+        // the bucket path meets each S word with R's sorted bucket of the
+        // same index, so there S is only bucketed, not moved (block-uniform)
+        const bool sort_s = ds.max_key || ones;
         if (ds.y_single) {
             for (uint32_t i = threadIdx.x; i < rslots; i += blockDim.x) {
                 const uint64_t v = A[i];   // pads are all-ones words: K < 0xFFFFFFFF never meets them
@@ -220,7 +231,12 @@ smj_items(SmjArgs a) {
             }
             __syncthreads();
         } else {
-            dual_sort_rest(ds, A, rslots, B, C, sslots, A, cnt, red32);
+            dual_sort_rest(ds, A, rslots, B, C, sslots, A, cnt, red32, sort_s);
+            if (ds.bitonic && !sort_s) {   // R took the bitonic path: the merge path needs S sorted too
+                for (uint32_t i = threadIdx.x; i < sslots; i += blockDim.x) A[i] = C[i];
+                __syncthreads();
+                bitonic_words(A, sslots);
+            }
         }
         const uint32_t nr = rslots - rpad, ns = sslots - spad;
         const uint64_t *Rs = B, *Ss = A;
@@ -242,9 +258,6 @@ smj_items(SmjArgs a) {
                 if (m < a.mat_cap) a.mat[m] = s;
             }
         };
-        // all-ones words beyond the pads: real tuples with key 0xFFFFFFFF
-        const bool ones = !ds.y_single && !ds.bitonic && (rslots - (ds.nb ? ds.ex[ds.nb - 1] : 0u) != rpad ||
-                                                          sslots - (ds.nb ? ds.ey[ds.nb - 1] : 0u) != spad);
         if (ds.y_single) {
             // the S block is one key K (a hot key under skew), left unsorted in C
             // with its pads: every S word but the pads meets R's run of K, B[0..runn[cur])
@@ -256,13 +269,15 @@ smj_items(SmjArgs a) {
                 bool have = false;
                 for (uint32_t t = 0; t < nrun; t++) emit(s, Rs[t], sh, have);
             }
-        } else if (!ds.bitonic && !ds.max_key && !ones) {
-            // both runs are ordered by the same buckets: S bucket d meets R bucket
-            // d, whose sorted range [ex[d - 1], ex[d]) holds every R tuple that
-            // can have the S tuple's key; no key is 0xFFFFFFFF, so no pad matches
+        } else if (!ds.bitonic && !sort_s) {
+            // S word s in bucket d meets R bucket d, whose sorted range
+            // [ex[d - 1], ex[d]) holds every R tuple that can have s's key; no
+            // key is 0xFFFFFFFF, so the all-ones words in the unsorted S block
+            // are exactly its pads and are skipped
             const uint16_t *cx = ds.ex;
-            for (uint32_t j = threadIdx.x; j < ns && warp != kCtl; j += kWork) {
-                const uint64_t s = Ss[j];
+            for (uint32_t j = threadIdx.x; j < sslots && warp != kCtl; j += kWork) {
+                const uint64_t s = C[j];
+                if (s == ~0ULL) continue;   // a pad
                 const uint32_t key = tkey(s);
                 const uint32_t d = ds.bucket(s);
                 uint64_t sh = 0;

@@ -156,6 +156,7 @@ struct DualSort {
                                  // (< 0xFFFFFFFF): Y is left unsorted in place, ey is not set
     uint32_t y_key;
     uint32_t all_and, vary;      // AND of all keys; key bits that differ (0: none)
+    uint32_t onesx, onesy;       // all-ones words in X / Y (pads included)
     const uint16_t *ex, *ey;     // end of bucket d of Xo / Yo: ex[d], ey[d] (unless bitonic)
     __device__ __forceinline__ uint32_t bucket(uint64_t v) const {
         return v == ~0ULL ? nb : (tkey(v) >> shift) & bmask;
@@ -169,9 +170,9 @@ __device__ __forceinline__ uint32_t inc16(uint32_t *w, uint32_t d) {
     return (atomicAdd(&w[d >> 1], 1u << sh) >> sh) & 0xFFFFu;
 }
 
-// Scratch words of red[] that dual_chunk_sort uses: [0, 192) the analysis,
+// Scratch words of red[] that dual_chunk_sort uses: [0, 224) the analysis,
 // [0, 32) the scan.
-constexpr uint32_t kDualRedWords = 192;
+constexpr uint32_t kDualRedWords = 224;
 
 // First half of dual_chunk_sort: the bucket function of X[0..nx) and
 // Y[0..ny) (the (at most) 11 highest key bits that differ within both) and
@@ -182,7 +183,7 @@ __device__ __forceinline__ DualSort dual_analyze(const uint64_t *X, uint32_t nx,
                                                  uint32_t *cnt, uint32_t *red, uint32_t ypads) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int nw = (int)(blockDim.x >> 5);
-    uint32_t a = 0xFFFFFFFFu, o = 0, mk = 0, ay = 0xFFFFFFFFu, oy = 0, onesy = 0;
+    uint32_t a = 0xFFFFFFFFu, o = 0, mk = 0, ay = 0xFFFFFFFFu, oy = 0, onesy = 0, onesx = 0;
     for (uint32_t i = threadIdx.x; i < nx + ny; i += blockDim.x) {
         const uint64_t v = i < nx ? X[i] : Y[i - nx];
         if (v != ~0ULL) {
@@ -195,6 +196,8 @@ __device__ __forceinline__ DualSort dual_analyze(const uint64_t *X, uint32_t nx,
             }
         } else if (i >= nx) {
             onesy++;
+        } else {
+            onesx++;
         }
     }
 #pragma unroll
@@ -205,10 +208,11 @@ __device__ __forceinline__ DualSort dual_analyze(const uint64_t *X, uint32_t nx,
         ay &= __shfl_xor_sync(0xffffffffu, ay, s);
         oy |= __shfl_xor_sync(0xffffffffu, oy, s);
         onesy += __shfl_xor_sync(0xffffffffu, onesy, s);
+        onesx += __shfl_xor_sync(0xffffffffu, onesx, s);
     }
     if (lane == 0) {
         red[wid] = a; red[32 + wid] = o; red[64 + wid] = mk;
-        red[96 + wid] = ay; red[128 + wid] = oy; red[160 + wid] = onesy;
+        red[96 + wid] = ay; red[128 + wid] = oy; red[160 + wid] = onesy; red[192 + wid] = onesx;
     }
     for (uint32_t d = threadIdx.x; d < kDualCntWords; d += blockDim.x) cnt[d] = 0;
     __syncthreads();
@@ -218,6 +222,7 @@ __device__ __forceinline__ DualSort dual_analyze(const uint64_t *X, uint32_t nx,
     ay = lane < nw ? red[96 + lane] : 0xFFFFFFFFu;
     oy = lane < nw ? red[128 + lane] : 0u;
     onesy = lane < nw ? red[160 + lane] : 0u;
+    onesx = lane < nw ? red[192 + lane] : 0u;
 #pragma unroll
     for (int s = 16; s > 0; s >>= 1) {
         a &= __shfl_xor_sync(0xffffffffu, a, s);
@@ -226,8 +231,11 @@ __device__ __forceinline__ DualSort dual_analyze(const uint64_t *X, uint32_t nx,
         ay &= __shfl_xor_sync(0xffffffffu, ay, s);
         oy |= __shfl_xor_sync(0xffffffffu, oy, s);
         onesy += __shfl_xor_sync(0xffffffffu, onesy, s);
+        onesx += __shfl_xor_sync(0xffffffffu, onesx, s);
     }
     DualSort r;
+    r.onesx = onesx;
+    r.onesy = onesy;
     // Y of one key: ay == oy over its non-pad words, none of them all-ones
     // beyond the pads (so no real key-0xFFFFFFFF tuple hides among the pads)
     r.y_single = ny > onesy && ay == oy && ay != 0xFFFFFFFFu && onesy == ypads;
@@ -251,15 +259,17 @@ __device__ __forceinline__ DualSort dual_analyze(const uint64_t *X, uint32_t nx,
 // Second half of dual_chunk_sort (every thread calls it right after
 // dual_analyze, with the same arguments): counts, one scan of both sides'
 // counters, scatter, then the order inside buckets that hold several keys.
+// sort_y = false (block-uniform) sorts X only: Y is neither counted nor moved
+// and ey is not set, for a caller that needs only Y's bucket of each word.
 __device__ __forceinline__ void dual_sort_rest(DualSort &r, const uint64_t *X, uint32_t nx, uint64_t *Xo,
                                                const uint64_t *Y, uint32_t ny, uint64_t *Yo, uint32_t *cnt,
-                                               uint32_t *red) {
+                                               uint32_t *red, bool sort_y = true) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int nw = (int)(blockDim.x >> 5);
     const uint32_t nb = r.nb, W = nb + 1;   // counters per side; [nb] = all-ones words
     uint32_t *wx = cnt, *wy = cnt + (W + 1) / 2;   // packed counter words of each side
     uint16_t *cx = reinterpret_cast<uint16_t *>(wx), *cy = reinterpret_cast<uint16_t *>(wy);
-    const uint32_t nyc = r.y_single ? 0u : ny;   // Y words counted and placed
+    const uint32_t nyc = r.y_single || !sort_y ? 0u : ny;   // Y words counted and placed
     for (uint32_t i = threadIdx.x; i < nx + nyc; i += blockDim.x) {
         if (i < nx) inc16(wx, r.bucket(X[i]));
         else inc16(wy, r.bucket(Y[i - nx]));
@@ -301,11 +311,13 @@ __device__ __forceinline__ void dual_sort_rest(DualSort &r, const uint64_t *X, u
         Xo[inc16(wx, r.bucket(v))] = v;
     }
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < nyc; i += blockDim.x) {
-        const uint64_t v = Y[i];
-        Yo[inc16(wy, r.bucket(v))] = v;
+    if (nyc) {   // block-uniform
+        for (uint32_t i = threadIdx.x; i < nyc; i += blockDim.x) {
+            const uint64_t v = Y[i];
+            Yo[inc16(wy, r.bucket(v))] = v;
+        }
+        __syncthreads();
     }
-    __syncthreads();
     // cx / cy[d] = end of bucket d.  Buckets that need whole-word order: all of
     // them when lower key bits vary; else only the bucket that can hold key
     // 0xFFFFFFFF (the last one, if every key bit outside the buckets is one).
@@ -316,13 +328,13 @@ __device__ __forceinline__ void dual_sort_rest(DualSort &r, const uint64_t *X, u
         int big = 0;
         for (uint32_t d = d_first + threadIdx.x; d < nb; d += blockDim.x) {
             if (cx[d] - (d ? cx[d - 1] : 0u) > 128) big |= 1;
-            if (cy[d] - (d ? cy[d - 1] : 0u) > 128) big |= 2;
+            if (nyc && cy[d] - (d ? cy[d - 1] : 0u) > 128) big |= 2;
         }
         bigx = __syncthreads_or(big & 1);
         bigy = __syncthreads_or(big & 2);
     }
     if ((!bigx || !bigy) && d_first < nb) {
-        const uint32_t sides = (bigx ? 0u : 1u) | (bigy ? 0u : 2u);
+        const uint32_t sides = (bigx ? 0u : 1u) | (bigy || !nyc ? 0u : 2u);
         for (uint32_t t = d_first + threadIdx.x; t < 2 * nb; t += blockDim.x) {
             if (t < nb) {
                 if (sides & 1) insertion_words(Xo, t ? cx[t - 1] : 0u, cx[t]);
