@@ -62,11 +62,11 @@ KERNELS = {
               1: ("partition_pass<1,512> (pass 2)", 16, (276288768 + 214363648) / 2**25),
               3: ("radix_join_items<Chain>", 8, (273622272 + 3668736) / 2**25)},
     "npo": {0: ("partition_pass<0,512,hashed> (grouping by table region)", 16, (540667392 + 486182144) / 2**26),
-            1: ("npo_build_pages", 8, (812259584 + 381960960) / 2**26),
-            3: ("npo_probe_pages", 8, (967028736 + 4030976) / 2**26)},
+            1: ("npo_build_pages", 8, (812415744 + 381705728) / 2**26),
+            3: ("npo_probe_pages", 8, (809180672 + 3512320) / 2**26)},
     "smj": {0: ("partition_pass (both passes)", 32,
                 (271074048 + 215111680 + 279591680 + 219554048) / 2**25),
-            3: ("smj_items", 8, (281787648 + 3820288) / 2**25)},
+            3: ("smj_items", 8, (282003456 + 3525376) / 2**25)},
 }
 
 
