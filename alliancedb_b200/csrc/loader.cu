@@ -60,23 +60,20 @@ static bool parse_long(const std::string &s, long lo, long hi, long *v) {
     return true;
 }
 
-// The reference's smooth(): for a run [cur, i) of equal values followed by a
-// different one, element cur + j gets j * (v[i] - v[cur]) / run added (the
-// difference taken in uint64, the step and the sum in double).
-static void smooth_ts(uint64_t *ret, uint64_t n) {
-    int step_size = 0;
-    uint64_t current_index = 0;
-    uint64_t head_ts = n ? ret[0] : 0;
-    for (uint64_t i = 0; i < n; i++) {
-        if (head_ts == ret[i]) {
-            step_size++;
-        } else {
-            const double inner_add = (double)(ret[i] - ret[current_index]) / (double)step_size;
-            for (int j = 0; j < step_size; j++) ret[current_index + j] = (uint64_t)((double)ret[current_index + j] + j * inner_add);
-            head_ts = ret[i];
-            current_index = i;
-            step_size = 1;
-        }
+// The reference's smooth(): a maximal run ts[b, i) of equal values that is
+// followed by a different value ts[i] is spread towards it: ts[b + k] becomes
+// (uint64)((double)ts[b + k] + k * d) with d = (double)(ts[i] - ts[b]) / len,
+// the difference taken in uint64 and the run length an int.  The k = 0 term
+// is kept: above 2^53 the round trip through double changes the value.  A
+// run at the end of the array stays as it is.
+static void smooth_ts(uint64_t *ts, uint64_t n) {
+    uint64_t b = 0;                      // start of the current run
+    for (uint64_t i = 1; i < n; i++) {
+        if (ts[i] == ts[b]) continue;
+        const int len = (int)(i - b);
+        const double d = (double)(ts[i] - ts[b]) / (double)len;
+        for (int k = 0; k < len; k++) ts[b + k] = (uint64_t)((double)ts[b + k] + k * d);
+        b = i;
     }
 }
 
