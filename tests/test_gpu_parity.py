@@ -225,3 +225,22 @@ def test_host_inputs_through_the_staged_copy(oracle, algo):
     Sv = S[1:]
     got = adb.join(algo, R, Sv)
     assert (got.count, got.checksum) == oracle.pk_truth(R, Sv)
+
+
+@pytest.mark.parametrize("algo", ["m-way", "m-way+skew"])
+@pytest.mark.parametrize("case", ["one_key", "many_keys", "max_key"])
+def test_sort_merge_small_r_large_s(oracle, algo, case):
+    """A small R against a large S: each partition has hundreds of S blocks against one R chunk (S
+    blocks of one key, S blocks of many keys joined by bucket, and blocks holding key 0xFFFFFFFF, which
+    take the merge path with S sorted)."""
+    R = adb.gen_pk(4096, 41)
+    n_s = 1 << 22
+    if case == "one_key":
+        S = adb.tuples(np.full(n_s, R["key"][7], np.uint32))
+    elif case == "many_keys":
+        S = adb.gen_fk(n_s, R, 0.9, 42)
+    else:
+        R["key"][:3] = 0xFFFFFFFF
+        keys = np.random.default_rng(43).choice(R["key"], n_s)
+        S = adb.tuples(keys.astype(np.uint32))
+    check(oracle, algo, R, S)
