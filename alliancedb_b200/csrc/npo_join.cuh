@@ -81,17 +81,32 @@ __device__ __forceinline__ void npo_window(const uint64_t *table, uint64_t mask,
     hi = __ldg(reinterpret_cast<const ulonglong2 *>(table + ((b + 2) & mask)));
 }
 
-// One probe: S tuple s with start slot `slot`, given its window (lo, hi, read
-// by npo_window).  The window is scanned from the start slot; only a probe
-// whose run of occupied slots reaches the window's end goes on slot by slot,
-// as linear probing does.  nsent = build tuples equal to the empty marker
-// (they match key 0xFFFFFFFF).
+// The slots after a probe's window: linear probing from slot
+// (slot & ~1) + 4 until the first empty slot, for a probe whose run of
+// occupied slots reached the window's end.
 template <bool kMaterialize>
-__device__ __forceinline__ void npo_probe_one(NpoSink<kMaterialize> &sink, const uint64_t *table, uint64_t mask,
-                                              uint64_t s, uint64_t slot, ulonglong2 lo, ulonglong2 hi,
-                                              uint64_t nsent) {
+__device__ __forceinline__ void npo_probe_rest(NpoSink<kMaterialize> &sink, const uint64_t *table, uint64_t mask,
+                                               uint64_t s, uint64_t slot, uint64_t sh) {
     const uint32_t key = tkey(s);
-    const uint64_t sh = s_half(key, tpay(s));
+    uint64_t sl = ((slot & ~1ULL) + 4) & mask;
+    for (uint64_t tries = 0; tries <= mask; tries++) {
+        const uint64_t v = table[sl];
+        if (v == kEmpty) break;
+        if (tkey(v) == key) sink.match(s, key, tpay(v), sh);
+        sl = (sl + 1) & mask;
+    }
+}
+
+// One probe's window: S tuple s with start slot `slot`, given its window
+// (lo, hi, read by npo_window), scanned from the start slot; the matches of
+// build tuples equal to the empty marker (nsent of them, key 0xFFFFFFFF) are
+// added here too.  Returns true when the run of occupied slots reaches the
+// window's end, so that npo_probe_rest must go on.
+template <bool kMaterialize>
+__device__ __forceinline__ bool npo_probe_window(NpoSink<kMaterialize> &sink, uint64_t s, uint64_t slot,
+                                                 ulonglong2 lo, ulonglong2 hi, uint64_t nsent, uint64_t &sh) {
+    const uint32_t key = tkey(s);
+    sh = s_half(key, tpay(s));
     const uint64_t w4[4] = {lo.x, lo.y, hi.x, hi.y};
     bool open = true;   // no empty slot met yet
     uint32_t hits = 0;  // matching slots of the window
@@ -108,15 +123,6 @@ __device__ __forceinline__ void npo_probe_one(NpoSink<kMaterialize> &sink, const
         const ulonglong2 h2 = j & 2 ? hi : lo;
         sink.match(s, key, tpay(j & 1 ? h2.y : h2.x), sh);
     }
-    if (open) {   // the run reaches the window's end: continue linear probing
-        uint64_t sl = ((slot & ~1ULL) + 4) & mask;
-        for (uint64_t tries = 0; tries <= mask; tries++) {
-            const uint64_t v = table[sl];
-            if (v == kEmpty) break;
-            if (tkey(v) == key) sink.match(s, key, tpay(v), sh);
-            sl = (sl + 1) & mask;
-        }
-    }
     if (key == 0xFFFFFFFFu && nsent) {
         sink.a.count += nsent;
         sink.a.sum += nsent * pair_hash_pre(key, 0xFFFFFFFFu, sh);
@@ -126,6 +132,16 @@ __device__ __forceinline__ void npo_probe_one(NpoSink<kMaterialize> &sink, const
                 if (k < sink.mat_cap) sink.mat[k] = s;
             }
     }
+    return open;
+}
+
+// One whole probe: the window, then the slots after it where needed.
+template <bool kMaterialize>
+__device__ __forceinline__ void npo_probe_one(NpoSink<kMaterialize> &sink, const uint64_t *table, uint64_t mask,
+                                              uint64_t s, uint64_t slot, ulonglong2 lo, ulonglong2 hi,
+                                              uint64_t nsent) {
+    uint64_t sh;
+    if (npo_probe_window(sink, s, slot, lo, hi, nsent, sh)) npo_probe_rest(sink, table, mask, s, slot, sh);
 }
 
 // Probe: each thread takes kProbeU S tuples at a time (a grid-stride group),
